@@ -1,0 +1,422 @@
+#!/usr/bin/env python3
+"""Benchmark of the LEVIATHAN core engine step on B200.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+Workload (one "step" = one engine step of the whole network): plain engine
+at scale -- seeded Watts-Strogatz N = 1,000,000, k = 32, p = 0.1 (E = 32 M
+directed edges), delays uniform in [1, 64], omega ~ N(0,1), theta ~ U[0,2pi),
+w ~ U[0,1), dt = 0.05, reference parameter defaults, controller on.
+Inputs (1.2 GB resident) exceed the 126 MB L2, so no flush is needed.
+
+Metric: edge-updates/s = E x steps / elapsed.
+* ``value``   -- device-resident throughput: K steps replayed from CUDA
+  graphs, timed with CUDA events on the engine stream, max over ranks.
+* ``e2e``     -- the whole job through the public API with host buffers:
+  ``LeviathanEngine(...)`` from host arrays (H2D), K x ``step(dt)`` each
+  returning r to the host, ``get_theta()`` (D2H), wall clock.
+* ``--impl reference`` runs the reference engine itself (its
+  leviathan_kernel.cu built from the reference sources for sm_100a, and its
+  stock 86;90 build, in oracle/_ref) through its C ABI on the same GPU, the
+  same job as ``e2e`` (the reference has no CPU implementation of the path).
+Multi-GPU: the single network does not shard; ``--gpus N`` runs N
+independent replicas (one per rank, distinct seeds), weak scaling.
+"""
+
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import time
+
+import numpy as np
+
+REPO = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, REPO)
+
+DT = 0.05
+WORKLOAD = dict(N=1_000_000, k=32, p=0.1, max_delay=64)
+WORKLOAD_NAME = ("plain engine at scale: Watts-Strogatz N=1e6, k=32, p=0.1, "
+                 "delays U[1,64], dt=0.05, controller on")
+
+
+# ---------------------------------------------------------------------------
+# helpers
+# ---------------------------------------------------------------------------
+def dist_env():
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return rank, world, local
+
+
+def init_dist(world, local):
+    import torch
+
+    if torch.cuda.is_available():
+        torch.cuda.set_device(local)
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+
+        dist.init_process_group("nccl" if torch.cuda.is_available() else "gloo",
+                                timeout=datetime.timedelta(seconds=600))
+
+
+def barrier(world):
+    if world > 1:
+        import torch
+        import torch.distributed as dist
+
+        if torch.cuda.is_available():
+            dist.barrier(device_ids=[torch.cuda.current_device()])
+        else:
+            dist.barrier()
+
+
+def max_over_ranks(x, world):
+    if world <= 1:
+        return float(x)
+    import torch
+    import torch.distributed as dist
+
+    dev = "cuda" if torch.cuda.is_available() else "cpu"
+    t = torch.tensor([float(x)], dtype=torch.float64, device=dev)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def sum_over_ranks(x, world):
+    if world <= 1:
+        return float(x)
+    import torch
+    import torch.distributed as dist
+
+    dev = "cuda" if torch.cuda.is_available() else "cpu"
+    t = torch.tensor([float(x)], dtype=torch.float64, device=dev)
+    dist.all_reduce(t, op=dist.ReduceOp.SUM)
+    return float(t.item())
+
+
+def measured_peaks():
+    path = os.path.join(REPO, "MEASURED_PEAKS.json")
+    if os.path.exists(path):
+        with open(path) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+def profiled_traffic(kernel="step_kernel"):
+    """DRAM bytes per launch of the step kernel from the committed ncu
+    summary (profiles/), or None."""
+    path = os.path.join(REPO, "profiles", f"{kernel}_traffic.txt")
+    if not os.path.exists(path):
+        return None
+    for line in open(path):
+        if line.startswith("dram_bytes_per_launch:"):
+            return float(line.split(":")[1])
+    return None
+
+
+class ClockSampler:
+    """nvidia-smi clock / throttle sampling while the timed region runs."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index):
+        self.idx = gpu_index
+        self.proc = None
+        self.path = f"/tmp/lev_clocks_{os.getpid()}.csv"
+
+    def start(self):
+        try:
+            self.f = open(self.path, "w")
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.idx}", f"--query-gpu={self.Q}",
+                 "--format=csv,noheader,nounits", "-lms", "50"],
+                stdout=self.f, stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+        return self
+
+    def stop(self):
+        if self.proc is None:
+            return None
+        time.sleep(0.1)
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        self.f.close()
+        rows = []
+        for line in open(self.path):
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                rows.append(dict(sm=float(parts[1]), max=float(parts[2]),
+                                 power=float(parts[3]),
+                                 hw=parts[5], hwt=parts[6], swt=parts[7], swp=parts[8]))
+            except ValueError:
+                continue
+        os.unlink(self.path)
+        if not rows:
+            return None
+        load = [r for r in rows if r["power"] > 250.0] or rows
+        reasons = set()
+        for r in load:
+            for k, name in (("hw", "hw_slowdown"), ("hwt", "hw_thermal_slowdown"),
+                            ("swt", "sw_thermal_slowdown"), ("swp", "sw_power_cap")):
+                if r[k].lower().startswith("active"):
+                    reasons.add(name)
+        return {"sm_mhz": statistics.median(r["sm"] for r in load),
+                "sm_max_mhz": max(r["max"] for r in rows),
+                "reasons": sorted(reasons), "samples": len(load)}
+
+
+def build_workload(seed):
+    from leviathan_v1_b200.graphs import make_network
+
+    return make_network(WORKLOAD["N"], WORKLOAD["k"], WORKLOAD["p"],
+                        WORKLOAD["max_delay"], seed)
+
+
+def algorithmic_bytes(N, E):
+    """Bytes one step must move (reference layout): per edge col 4 + delay 1
+    + weight read 4 + weight write 4 + delayed-phase gather 4 = 17; per node
+    row_ptr 4 + theta r/w 8 + theta_hat r/w 8 + omega 4 + omega_hat r/w 8 +
+    ring-slot write 4 = 36; plus row_ptr[N]."""
+    return 17 * E + 36 * N + 4
+
+
+def cpu_baseline(net, budget_s=20.0):
+    """FP64 NumPy oracle (oracle/oracle64.py) on the host: a bounded sample
+    of steps of the same network."""
+    sys.path.insert(0, os.path.join(REPO, "oracle"))
+    from oracle64 import OracleEngine
+
+    o = OracleEngine(*net.engine_args())
+    t0 = time.perf_counter()
+    o.step(DT)  # first step: warm caches, allocations
+    first = time.perf_counter() - t0
+    n = max(1, min(50, int(budget_s / max(first, 1e-3))))
+    t0 = time.perf_counter()
+    for _ in range(n):
+        o.step(DT)
+    el = time.perf_counter() - t0
+    return {"value": net.E * n / el, "unit": "edge-updates/s", "cores": 1,
+            "kind": "port",
+            "sample": f"{n} steps (after 1 warm-up step) of the bench network, "
+                      f"FP64 NumPy oracle, single-threaded NumPy, "
+                      f"{os.cpu_count()} host cores present"}
+
+
+def fp64_error_small():
+    """Wrapped-phase error after 200 steps against the FP64 oracle on the
+    small configuration (N=1000, k=20), both math modes."""
+    sys.path.insert(0, os.path.join(REPO, "oracle"))
+    from oracle64 import OracleEngine, circular_distance
+
+    from leviathan_v1_b200 import LeviathanEngine
+    from leviathan_v1_b200.graphs import config_small
+
+    net = config_small(0)
+    o = OracleEngine(*net.engine_args())
+    o.run(DT, 200)
+    out = {}
+    for mode in ("reference", "accurate"):
+        e = LeviathanEngine(*net.engine_args(), math_mode=mode)
+        e.step_n(DT, 200)
+        out[mode] = float(circular_distance(e.get_theta(), o.theta).max())
+        e.close()
+    return out
+
+
+# ---------------------------------------------------------------------------
+# our engine
+# ---------------------------------------------------------------------------
+def run_ours(args, rank, world, local):
+    import torch
+
+    from leviathan_v1_b200 import LeviathanEngine
+
+    net = build_workload(seed=rank)
+    N, E = net.N, net.E
+    K, W = args.steps, args.warmup
+
+    eng = LeviathanEngine(*net.engine_args())
+    stream = torch.cuda.ExternalStream(eng.stream_ptr)
+    sampler = ClockSampler(torch.cuda.current_device()).start()
+
+    # warm-up: graphs instantiated for the block lengths used below
+    eng.step_n_async(DT, W)
+    eng.step_n_async(DT, K)
+    eng.synchronize()
+
+    barrier(world)
+    torch.cuda.synchronize()
+    ev0 = torch.cuda.Event(enable_timing=True)
+    ev1 = torch.cuda.Event(enable_timing=True)
+    ev0.record(stream)
+    eng.step_n_async(DT, K)
+    ev1.record(stream)
+    ev1.synchronize()
+    torch.cuda.synchronize()
+    barrier(world)
+    ms = ev0.elapsed_time(ev1)
+    clocks = sampler.stop()
+    ms_max = max_over_ranks(ms, world)
+    edges_total = sum_over_ranks(E, world)
+    value = edges_total * K / (ms_max / 1e3)
+    r_last = eng.get_r()
+    eng.close()
+
+    # end-to-end through the public API with host buffers
+    barrier(world)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    e2 = LeviathanEngine(*net.engine_args())
+    for _ in range(K):
+        e2.step(DT)
+    theta = e2.get_theta()
+    torch.cuda.synchronize()
+    e2e_s = time.perf_counter() - t0
+    e2.close()
+    e2e_s = max_over_ranks(e2e_s, world)
+    h2d = (N + 1) * 4 + E * (4 + 1 + 4) + N * 4 * 3
+    d2h = 4 * K + 4 * N
+    e2e = {"value": edges_total * K / e2e_s, "unit": "edge-updates/s",
+           "h2d_bytes_per_step": h2d / K, "d2h_bytes_per_step": d2h / K,
+           "path": "LeviathanEngine(host arrays) + K x step(dt)->r + get_theta()",
+           "seconds": e2e_s}
+
+    step_s = ms / 1e3 / K
+    alg = algorithmic_bytes(N, E)
+    peak, peak_kind = measured_peaks()
+    achieved = alg / step_s / 1e9
+    traffic = profiled_traffic()
+    line = {
+        "metric": "edge-updates/s", "value": value, "unit": "edge-updates/s",
+        "n_gpus": world, "steps": K, "warmup": W, "ms_per_step": ms_max / K,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f32", "data": "synthetic (seeded Watts-Strogatz, seeded states)",
+        "config": {"workload": WORKLOAD_NAME, "N": N, "E": E,
+                   "max_delay": WORKLOAD["max_delay"], "dt": DT,
+                   "parallelism": f"replicas x{world} (single network does not shard)",
+                   "l2": "inputs (1.2 GB) larger than L2 (126 MB); no flush"},
+        "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak,
+                     "unit": "GB/s", "frac": achieved / peak, "peak_kind": peak_kind,
+                     "traffic": traffic, "kernel": "lev::step_kernel<0>",
+                     "algorithmic_bytes_per_launch": alg},
+        "e2e": e2e,
+        "gpu_launches": K + (K + 255) // 256,
+        "clocks": clocks,
+        "r_final": r_last,
+        "theta_finite": bool(np.all(np.isfinite(theta))),
+    }
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        line["cpu_baseline"] = cpu_baseline(net, budget_s=args.cpu_budget)
+    if rank == 0 and not args.no_fp64_check:
+        line["fp64_error_small_200_steps"] = fp64_error_small()
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+
+
+# ---------------------------------------------------------------------------
+# reference engine (oracle/_ref, built from the reference sources)
+# ---------------------------------------------------------------------------
+def run_reference(args, rank, world, local):
+    if rank != 0:
+        return
+    import torch
+
+    sys.path.insert(0, os.path.join(REPO, "oracle"))
+    import refengine
+
+    net = build_workload(seed=0)
+    K, W = args.steps, args.warmup
+    results = {}
+    for flavor in ("sm100a", "stock"):
+        if not refengine.available(flavor):
+            continue
+        # warm-up run (JIT of the stock build, allocations)
+        ref = refengine.RefEngine(*net.engine_args(), flavor=flavor)
+        for _ in range(W):
+            ref.step(DT)
+        ref.close()
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        ref = refengine.RefEngine(*net.engine_args(), flavor=flavor)
+        for _ in range(K):
+            ref.step(DT)
+        ref.get_theta()
+        torch.cuda.synchronize()
+        el = time.perf_counter() - t0
+        ref.close()
+        results[flavor] = net.E * K / el
+    if not results:
+        print(json.dumps({"impl": "reference", "unavailable":
+                          "oracle/_ref reference build missing (make -C oracle)"}))
+        return
+    best = max(results, key=results.get)
+    v = results[best]
+    line = {
+        "impl": "reference", "metric": "edge-updates/s", "value": v,
+        "unit": "edge-updates/s", "n_gpus": 1, "steps": K, "warmup": W,
+        "ms_per_step": net.E / v * 1e3, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+        "data": "synthetic (seeded Watts-Strogatz, seeded states)",
+        "config": {"workload": WORKLOAD_NAME, "N": net.N, "E": net.E,
+                   "max_delay": WORKLOAD["max_delay"], "dt": DT,
+                   "parallelism": "single GPU (rank 0)"},
+        "reference_builds": results, "reference_build_used": best,
+        "e2e": {"value": v, "unit": "edge-updates/s", "h2d_bytes_per_step": 0,
+                "d2h_bytes_per_step": 0},
+        "cpu_baseline": {"value": v, "unit": "edge-updates/s", "cores": 1,
+                         "kind": "reference",
+                         "sample": "the reference engine itself (leviathan_init + K x "
+                                   "leviathan_step + leviathan_get_theta) on the same "
+                                   "B200, one host thread; the reference implements "
+                                   "the path only in CUDA"},
+        "gpu_launches": 4 * K,
+    }
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=2000)
+    ap.add_argument("--warmup", type=int, default=20)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--cpu-budget", type=float, default=20.0)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-fp64-check", action="store_true")
+    args = ap.parse_args()
+    if args.warmup < 3:
+        args.warmup = 3
+    rank, world, local = dist_env()
+    init_dist(world, local)
+    try:
+        if args.impl == "reference":
+            run_reference(args, rank, world, local)
+        else:
+            run_ours(args, rank, world, local)
+    finally:
+        if world > 1:
+            import torch.distributed as dist
+
+            dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,255 @@
+/*
+ * leviathan_b200.h -- C ABI of the B200 engine for the delayed Kuramoto
+ * network with prediction-gated Hebbian plasticity and a homeostatic gain
+ * controller (LEVIATHAN core engine step).
+ *
+ * Two layers are exported by libleviathan_b200.so:
+ *
+ *  1. The reference's own C ABI, symbol for symbol (leviathan_init ...
+ *     leviathan_free).  A binding written against the reference
+ *     (src/bindings/leviathan_pybind11.cpp:10-25) links against this library
+ *     unchanged.  Unlike the reference, no call ever terminates the process:
+ *     failures are recorded and readable through lev_last_error().
+ *
+ *  2. The lev_* status-code ABI.  Every function returns LEV_OK (0) or a
+ *     negative LEV_ERR_* code; lev_last_error() returns a message for the
+ *     calling thread.  It adds batched networks (many independent networks in
+ *     one launch), step blocks (n steps per call, CUDA-graph replayed), full
+ *     state checkpoint / restore and per-network parameters.
+ *
+ * Plain pointers and sizes only; all host pointers are borrowed for the
+ * duration of the call.  Device pointers appear only in the *_dev functions.
+ * A handle is not thread-safe: concurrent calls on one handle are not
+ * supported (same as the reference).
+ */
+#ifndef LEVIATHAN_B200_H
+#define LEVIATHAN_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+#include <stdbool.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ------------------------------------------------------------------------ */
+/* Status codes                                                              */
+/* ------------------------------------------------------------------------ */
+#define LEV_OK 0
+#define LEV_ERR_ARG (-1)     /* invalid argument (size, range, null)        */
+#define LEV_ERR_CUDA (-2)    /* CUDA runtime error                          */
+#define LEV_ERR_STATE (-3)   /* call not valid in the current handle state  */
+#define LEV_ERR_NOMEM (-4)   /* device or host allocation failed            */
+
+/* Arithmetic of the transcendental calls inside the step.
+ * LEV_MATH_REFERENCE uses the same fast sin/cos intrinsic as the reference
+ * kernels (leviathan_kernel.cu:152,195) so results track the reference
+ * engine; LEV_MATH_ACCURATE uses correctly-ranged sincosf for the edge and
+ * order-parameter terms (lower error against an FP64 transcription). */
+#define LEV_MATH_REFERENCE 0
+#define LEV_MATH_ACCURATE 1
+
+/* Physics parameters of one network.  Defaults (lev_default_params) are the
+ * constants hard-coded in leviathan_init (leviathan_kernel.cu:282-296) and
+ * the literal g_rest = 1.5 of leviathan_step (leviathan_kernel.cu:433). */
+typedef struct LevParams {
+  float eta;       /* Hebbian learning rate                 (0.01)  */
+  float lam;       /* weight decay                          (0.001) */
+  float gamma;     /* prediction-error gating               (0.05)  */
+  float alpha_eps; /* prediction-error feedback on phase    (0.1)   */
+  float kappa_w;   /* predictor frequency adaptation        (0.01)  */
+  float w_min;     /* weight clamp                          (0.0)   */
+  float w_max;     /*                                       (2.0)   */
+  float g;         /* initial global coupling gain          (1.5)   */
+  float r0;        /* controller target order parameter     (0.5)   */
+  float beta;      /* controller gain rate                  (0.01)  */
+  float mu;        /* controller relaxation rate            (0.01)  */
+  float g_rest;    /* controller resting gain               (1.5)   */
+  float g_min;     /* gain clamp                            (0.1)   */
+  float g_max;     /*                                       (5.0)   */
+  int32_t gain_controller; /* 1 = on (default), 0 = off             */
+  int32_t reserved;
+} LevParams;
+
+typedef struct LevEngine LevEngine;
+
+/* Message of the last failed lev_* / leviathan_* call on this thread. */
+const char *lev_last_error(void);
+
+/* Library version string. */
+const char *lev_version(void);
+
+/* Fill *p with the reference defaults. */
+void lev_default_params(LevParams *p);
+
+/* ------------------------------------------------------------------------ */
+/* Construction                                                              */
+/* ------------------------------------------------------------------------ */
+
+/* One network.  Replaces leviathan_init (leviathan_kernel.cu:270-389).
+ * E = row_ptr[N].  Arrays: row_ptr[N+1] (non-decreasing, row_ptr[0]=0),
+ * col_idx[E] in [0,N), delays[E] in [0,max_delay], weights[E], theta[N],
+ * theta_hat[N], omega[N].  omega_hat starts equal to omega
+ * (leviathan_kernel.cu:350); every ring slot starts equal to theta
+ * (init_buffer_kernel, leviathan_kernel.cu:79-90).  max_delay in [0,255]
+ * (delays are uint8), N in [1, 2^24).  params may be NULL (defaults).
+ * math_mode is LEV_MATH_REFERENCE or LEV_MATH_ACCURATE.  The engine runs on
+ * the CUDA device that is current at the call. */
+int lev_create(LevEngine **out, int32_t N, int32_t max_delay,
+               const int32_t *row_ptr, const int32_t *col_idx,
+               const uint8_t *delays, const float *weights,
+               const float *theta, const float *theta_hat,
+               const float *omega, const LevParams *params,
+               int32_t math_mode);
+
+/* Many independent networks in one engine (packed CSR with per-network
+ * offsets).  No reference counterpart: the reference runs one engine per
+ * network (experiments/phase_sweep.py:25-59 drives one network serially).
+ * Arrays are the per-network arrays concatenated in network order:
+ * row_ptr_cat holds num_nets local row_ptr arrays of N[n]+1 entries each
+ * (values local to the network), the edge arrays hold sum(E[n]) entries,
+ * the node arrays sum(N[n]).  params holds num_nets entries (NULL: all
+ * defaults). */
+int lev_batch_create(LevEngine **out, int32_t num_nets, const int32_t *N,
+                     const int32_t *max_delay, const int32_t *row_ptr_cat,
+                     const int32_t *col_idx_cat, const uint8_t *delays_cat,
+                     const float *weights_cat, const float *theta_cat,
+                     const float *theta_hat_cat, const float *omega_cat,
+                     const LevParams *params, int32_t math_mode);
+
+/* Replaces leviathan_free (leviathan_kernel.cu:455-478). */
+int lev_destroy(LevEngine *h);
+
+/* Shape queries. */
+int lev_num_nets(const LevEngine *h, int32_t *out);
+int lev_total_nodes(const LevEngine *h, int64_t *out);
+int lev_total_edges(const LevEngine *h, int64_t *out);
+int lev_net_shape(const LevEngine *h, int32_t net, int32_t *N, int64_t *E,
+                  int32_t *max_delay);
+
+/* ------------------------------------------------------------------------ */
+/* Stepping                                                                  */
+/* ------------------------------------------------------------------------ */
+
+/* One step of every network.  Replaces leviathan_step
+ * (leviathan_kernel.cu:391-438): predictor, delayed gather + coupling +
+ * Hebbian update, integration + ring write, order parameter r, gain
+ * controller.  r_out[num_nets] receives r of theta(t+1) per network
+ * (may be NULL).  Synchronous, like the reference. */
+int lev_step(LevEngine *h, float dt, float *r_out);
+
+/* n steps of every network in one call; the step loop is replayed from a
+ * CUDA graph.  r_out[n*num_nets] (step-major) receives r per step and
+ * network (may be NULL).  Synchronous. */
+int lev_step_n(LevEngine *h, float dt, int32_t n, float *r_out);
+
+/* Asynchronous variant of lev_step_n for timing and device-side pipelines:
+ * enqueues n steps on the engine stream and returns.  r values stay on the
+ * device; lev_sync waits for completion. */
+int lev_step_n_async(LevEngine *h, float dt, int32_t n);
+int lev_sync(LevEngine *h);
+
+/* Engine stream as a cudaStream_t cast to void*. */
+int lev_get_stream(LevEngine *h, void **stream);
+
+/* ------------------------------------------------------------------------ */
+/* State access                                                              */
+/* ------------------------------------------------------------------------ */
+
+/* theta of all nodes (concatenated over networks).  Replaces
+ * leviathan_get_theta (leviathan_kernel.cu:440-443). */
+int lev_get_theta(LevEngine *h, float *theta_out);
+
+/* Upload theta of all nodes and refill every ring slot with it (θ̂, ω̂, w
+ * untouched).  Replaces leviathan_set_theta (leviathan_kernel.cu:445-453). */
+int lev_set_theta(LevEngine *h, const float *theta_in);
+
+/* Per-network variants (n in [0,num_nets)). */
+int lev_get_theta_net(LevEngine *h, int32_t net, float *theta_out);
+int lev_set_theta_net(LevEngine *h, int32_t net, const float *theta_in);
+
+/* Edge weights (concatenated).  lev_reset_weights replaces
+ * leviathan_reset_weights (leviathan_kernel.cu:492-497). */
+int lev_get_weights(LevEngine *h, float *w_out);
+int lev_reset_weights(LevEngine *h, const float *w_in);
+
+/* Predictor state (concatenated): theta_hat, omega_hat; and omega. */
+int lev_get_predictor(LevEngine *h, float *theta_hat_out,
+                      float *omega_hat_out);
+int lev_set_predictor(LevEngine *h, const float *theta_hat_in,
+                      const float *omega_hat_in);
+int lev_get_omega(LevEngine *h, float *omega_out);
+int lev_set_omega(LevEngine *h, const float *omega_in);
+
+/* Delay ring of one network exported in the reference layout:
+ * ring_out[N*(max_delay+1)], node-major, slot s of node j at
+ * ring_out[j*(max_delay+1)+s], slot of theta(t) = t mod (max_delay+1)
+ * (leviathan_kernel.cu:142-143,192).  *buf_idx receives that slot index. */
+int lev_get_ring(LevEngine *h, int32_t net, float *ring_out,
+                 int32_t *buf_idx);
+/* Inverse of lev_get_ring: restores the ring and the slot index. */
+int lev_set_ring(LevEngine *h, int32_t net, const float *ring_in,
+                 int32_t buf_idx);
+
+/* Steps taken by a network since creation. */
+int lev_get_step_count(LevEngine *h, int32_t net, int64_t *t);
+
+/* Gain g and last order parameter r of a network.  Replace
+ * leviathan_set_gain / leviathan_get_gain (leviathan_kernel.cu:480-482). */
+int lev_set_gain(LevEngine *h, int32_t net, float g);
+int lev_get_gain(LevEngine *h, int32_t net, float *g);
+int lev_get_r(LevEngine *h, int32_t net, float *r);
+
+/* Replaces leviathan_set_gain_controller (leviathan_kernel.cu:484-486). */
+int lev_set_gain_controller(LevEngine *h, int32_t net, int32_t enabled);
+
+/* Parameters of one network (net = -1: all networks). */
+int lev_set_params(LevEngine *h, int32_t net, const LevParams *p);
+int lev_get_params(LevEngine *h, int32_t net, LevParams *p);
+
+/* Arithmetic mode (LEV_MATH_*), switchable between steps. */
+int lev_set_math_mode(LevEngine *h, int32_t math_mode);
+
+/* Device bytes held by the engine.  Replaces leviathan_get_vram_usage
+ * (leviathan_kernel.cu:488-490), which returns a formula; this returns the
+ * bytes actually allocated. */
+int lev_get_vram_usage(const LevEngine *h, size_t *bytes);
+
+/* ------------------------------------------------------------------------ */
+/* Reference C ABI (leviathan_kernel.cu:21-499), same symbols and signatures */
+/* ------------------------------------------------------------------------ */
+typedef struct LeviathanHandle LeviathanHandle;
+
+/* leviathan_kernel.cu:270.  Returns NULL on failure (reference: exit(1)). */
+LeviathanHandle *leviathan_init(int N, int max_delay, int *h_row_ptr,
+                                int *h_col_idx, uint8_t *h_delays,
+                                float *h_weights, float *h_theta,
+                                float *h_theta_hat, float *h_omega);
+/* leviathan_kernel.cu:391.  Returns NaN on failure. */
+float leviathan_step(LeviathanHandle *handle, float dt);
+/* leviathan_kernel.cu:440 */
+void leviathan_get_theta(LeviathanHandle *handle, float *h_theta);
+/* leviathan_kernel.cu:445 */
+void leviathan_set_theta(LeviathanHandle *handle, float *h_theta);
+/* leviathan_kernel.cu:455 */
+void leviathan_free(LeviathanHandle *handle);
+/* leviathan_kernel.cu:480 */
+void leviathan_set_gain(LeviathanHandle *handle, float g);
+/* leviathan_kernel.cu:482 */
+float leviathan_get_gain(LeviathanHandle *handle);
+/* leviathan_kernel.cu:484 */
+void leviathan_set_gain_controller(LeviathanHandle *handle, bool enabled);
+/* leviathan_kernel.cu:488 */
+size_t leviathan_get_vram_usage(LeviathanHandle *handle);
+/* leviathan_kernel.cu:492 */
+void leviathan_reset_weights(LeviathanHandle *handle, float *h_weights);
+
+/* The engine behind a reference-ABI handle (for mixing both layers). */
+LevEngine *leviathan_engine(LeviathanHandle *handle);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* LEVIATHAN_B200_H */

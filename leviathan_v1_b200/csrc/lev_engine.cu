@@ -1,0 +1,1092 @@
+// lev_engine.cu -- host side of the C ABI declared in include/leviathan_b200.h.
+//
+// Owns device memory, the engine stream, the tile list and the CUDA graphs of
+// step blocks.  Replaces the host API of the reference engine
+// (leviathan_kernel.cu:266-499): every failure returns a status code and
+// leaves a message for lev_last_error(); nothing terminates the process.
+
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <limits>
+#include <map>
+#include <string>
+#include <tuple>
+#include <vector>
+
+#include "leviathan_b200.h"
+#include "lev_kernels.cuh"
+
+namespace lev {
+
+static thread_local std::string g_last_error;
+
+static int fail(int code, const std::string &msg) {
+  g_last_error = msg;
+  return code;
+}
+
+#define LEV_TRY_CUDA(call)                                                  \
+  do {                                                                      \
+    cudaError_t _e = (call);                                                \
+    if (_e != cudaSuccess)                                                  \
+      return fail(LEV_ERR_CUDA, std::string(#call) + " failed: " +          \
+                                    cudaGetErrorString(_e));                \
+  } while (0)
+
+// Makes the engine's device current for the scope of an API call and puts
+// the caller's device back afterwards.
+struct DeviceScope {
+  int prev = -1;
+  bool switched = false;
+  explicit DeviceScope(int dev) {
+    if (cudaGetDevice(&prev) == cudaSuccess && prev != dev) {
+      switched = (cudaSetDevice(dev) == cudaSuccess);
+    }
+  }
+  ~DeviceScope() {
+    if (switched) cudaSetDevice(prev);
+  }
+};
+
+struct GraphEntry {
+  cudaGraph_t graph = nullptr;
+  cudaGraphExec_t exec = nullptr;
+};
+
+}  // namespace lev
+
+using namespace lev;
+
+struct LevEngine {
+  int device = 0;
+  cudaStream_t stream = nullptr;
+  int num_nets = 0;
+  long long total_nodes = 0;
+  long long total_edges = 0;   // sum of E
+  long long edge_alloc = 0;    // padded edge allocation (multiple of 4, +4)
+  long long rp_total = 0;
+  long long ring_floats = 0;
+  int total_tiles = 0;
+  int math_mode = LEV_MATH_REFERENCE;
+  size_t vram = 0;
+
+  std::vector<NetDesc> h_nets;
+  std::vector<long long> net_E;
+
+  NetDesc *d_nets = nullptr;
+  NetState *d_st = nullptr;
+  int2 *d_tiles = nullptr;
+  int *d_row_ptr = nullptr;
+  uint32_t *d_cd = nullptr;
+  float *d_w = nullptr;
+  float *d_theta = nullptr;
+  float *d_theta_hat = nullptr;
+  float *d_omega = nullptr;
+  float *d_omega_hat = nullptr;
+  float *d_ring = nullptr;
+  float2 *d_part = nullptr;
+
+  // r of the last single step, written by the kernel into mapped host memory
+  float *h_rmap = nullptr;
+  float *d_rmap = nullptr;
+
+  // r history of step blocks
+  int block_len = 256;
+  float *d_rhist = nullptr;   // [block_len][num_nets]
+  float *h_rstage = nullptr;  // pinned staging for lev_step_n
+  size_t h_rstage_len = 0;
+
+  std::map<std::tuple<int, uint32_t, int>, GraphEntry> graphs;
+};
+
+struct LeviathanHandle {
+  LevEngine *eng;
+};
+
+namespace {
+
+template <typename T>
+int dev_alloc(LevEngine *h, T **p, size_t count) {
+  size_t bytes = std::max<size_t>(count, 1) * sizeof(T);
+  cudaError_t e = cudaMalloc(reinterpret_cast<void **>(p), bytes);
+  if (e != cudaSuccess) {
+    *p = nullptr;
+    return fail(LEV_ERR_NOMEM, std::string("cudaMalloc of ") +
+                                   std::to_string(bytes) + " bytes failed: " +
+                                   cudaGetErrorString(e));
+  }
+  h->vram += bytes;
+  return LEV_OK;
+}
+
+void free_engine(LevEngine *h) {
+  if (!h) return;
+  for (auto &kv : h->graphs) {
+    if (kv.second.exec) cudaGraphExecDestroy(kv.second.exec);
+    if (kv.second.graph) cudaGraphDestroy(kv.second.graph);
+  }
+  h->graphs.clear();
+  cudaFree(h->d_nets);
+  cudaFree(h->d_st);
+  cudaFree(h->d_tiles);
+  cudaFree(h->d_row_ptr);
+  cudaFree(h->d_cd);
+  cudaFree(h->d_w);
+  cudaFree(h->d_theta);
+  cudaFree(h->d_theta_hat);
+  cudaFree(h->d_omega);
+  cudaFree(h->d_omega_hat);
+  cudaFree(h->d_ring);
+  cudaFree(h->d_part);
+  cudaFree(h->d_rhist);
+  if (h->h_rmap) cudaFreeHost(h->h_rmap);
+  if (h->h_rstage) cudaFreeHost(h->h_rstage);
+  if (h->stream) cudaStreamDestroy(h->stream);
+  delete h;
+}
+
+void params_to_desc(const LevParams &p, NetDesc *d) {
+  d->eta = p.eta;
+  d->lam = p.lam;
+  d->gamma = p.gamma;
+  d->alpha = p.alpha_eps;
+  d->kappa_w = p.kappa_w;
+  d->w_min = p.w_min;
+  d->w_max = p.w_max;
+  d->r0 = p.r0;
+  d->beta = p.beta;
+  d->mu = p.mu;
+  d->g_rest = p.g_rest;
+  d->g_min = p.g_min;
+  d->g_max = p.g_max;
+  d->ctrl = p.gain_controller ? 1 : 0;
+}
+
+void desc_to_params(const NetDesc &d, float g, LevParams *p) {
+  p->eta = d.eta;
+  p->lam = d.lam;
+  p->gamma = d.gamma;
+  p->alpha_eps = d.alpha;
+  p->kappa_w = d.kappa_w;
+  p->w_min = d.w_min;
+  p->w_max = d.w_max;
+  p->g = g;
+  p->r0 = d.r0;
+  p->beta = d.beta;
+  p->mu = d.mu;
+  p->g_rest = d.g_rest;
+  p->g_min = d.g_min;
+  p->g_max = d.g_max;
+  p->gain_controller = d.ctrl;
+  p->reserved = 0;
+}
+
+int check_params(const LevParams &p) {
+  const float v[] = {p.eta, p.lam, p.gamma, p.alpha_eps, p.kappa_w,
+                     p.w_min, p.w_max, p.g, p.r0, p.beta,
+                     p.mu, p.g_rest, p.g_min, p.g_max};
+  for (float x : v)
+    if (!std::isfinite(x)) return fail(LEV_ERR_ARG, "parameter is not finite");
+  if (p.w_min > p.w_max) return fail(LEV_ERR_ARG, "w_min > w_max");
+  if (p.g_min > p.g_max) return fail(LEV_ERR_ARG, "g_min > g_max");
+  return LEV_OK;
+}
+
+int launch_fill(LevEngine *h, int n) {
+  const NetDesc &nd = h->h_nets[n];
+  const long long total = (long long)nd.bsi * nd.N;
+  int blocks = (int)std::min<long long>((total + 255) / 256, 148LL * 16);
+  ring_fill_kernel<<<blocks, 256, 0, h->stream>>>(
+      h->d_theta + nd.node_off, h->d_ring + nd.ring_off, nd.N, nd.Np, nd.bsi);
+  LEV_TRY_CUDA(cudaGetLastError());
+  return LEV_OK;
+}
+
+StepArgs make_args(LevEngine *h, float dt, float *r_hist, int r_cap,
+                   float *r_host) {
+  StepArgs a;
+  a.nets = h->d_nets;
+  a.st = h->d_st;
+  a.tiles = h->d_tiles;
+  a.row_ptr = h->d_row_ptr;
+  a.cd = h->d_cd;
+  a.w = h->d_w;
+  a.theta = h->d_theta;
+  a.theta_hat = h->d_theta_hat;
+  a.omega = h->d_omega;
+  a.omega_hat = h->d_omega_hat;
+  a.ring = h->d_ring;
+  a.partials = h->d_part;
+  a.r_hist = r_hist;
+  a.r_host = r_host;
+  a.r_cap = r_cap;
+  a.num_nets = h->num_nets;
+  a.dt = dt;
+  return a;
+}
+
+int launch_step(LevEngine *h, const StepArgs &a) {
+  if (h->math_mode == LEV_MATH_ACCURATE)
+    step_kernel<1><<<h->total_tiles, kTile, 0, h->stream>>>(a);
+  else
+    step_kernel<0><<<h->total_tiles, kTile, 0, h->stream>>>(a);
+  LEV_TRY_CUDA(cudaGetLastError());
+  return LEV_OK;
+}
+
+// Graph of `len` steps (r history rows 0..len-1) keyed by (len, dt, mode).
+int get_graph(LevEngine *h, int len, float dt, cudaGraphExec_t *out) {
+  uint32_t dbits;
+  std::memcpy(&dbits, &dt, 4);
+  auto key = std::make_tuple(len, dbits, h->math_mode);
+  auto it = h->graphs.find(key);
+  if (it != h->graphs.end()) {
+    *out = it->second.exec;
+    return LEV_OK;
+  }
+  if (h->graphs.size() >= 16) {
+    for (auto &kv : h->graphs) {
+      cudaGraphExecDestroy(kv.second.exec);
+      cudaGraphDestroy(kv.second.graph);
+    }
+    h->graphs.clear();
+  }
+  GraphEntry ge;
+  LEV_TRY_CUDA(
+      cudaStreamBeginCapture(h->stream, cudaStreamCaptureModeThreadLocal));
+  reset_rpos_kernel<<<1, 128, 0, h->stream>>>(h->d_st, h->num_nets);
+  StepArgs a = make_args(h, dt, h->d_rhist, h->block_len, nullptr);
+  int rc = LEV_OK;
+  for (int i = 0; i < len && rc == LEV_OK; ++i) rc = launch_step(h, a);
+  cudaError_t ce = cudaStreamEndCapture(h->stream, &ge.graph);
+  if (rc != LEV_OK) {
+    if (ge.graph) cudaGraphDestroy(ge.graph);
+    return rc;
+  }
+  if (ce != cudaSuccess)
+    return fail(LEV_ERR_CUDA,
+                std::string("graph capture failed: ") + cudaGetErrorString(ce));
+  ce = cudaGraphInstantiate(&ge.exec, ge.graph, 0);
+  if (ce != cudaSuccess) {
+    cudaGraphDestroy(ge.graph);
+    return fail(LEV_ERR_CUDA, std::string("graph instantiate failed: ") +
+                                  cudaGetErrorString(ce));
+  }
+  h->graphs[key] = ge;
+  *out = ge.exec;
+  return LEV_OK;
+}
+
+// Enqueue n steps as graph replays; if stage != null, the r history of every
+// block is copied into stage[n][num_nets] (pinned host memory).
+int enqueue_steps(LevEngine *h, float dt, int n, float *stage) {
+  int done = 0;
+  while (done < n) {
+    const int len = std::min(h->block_len, n - done);
+    cudaGraphExec_t ex;
+    int rc = get_graph(h, len, dt, &ex);
+    if (rc != LEV_OK) return rc;
+    LEV_TRY_CUDA(cudaGraphLaunch(ex, h->stream));
+    if (stage) {
+      LEV_TRY_CUDA(cudaMemcpyAsync(
+          stage + (size_t)done * h->num_nets, h->d_rhist,
+          sizeof(float) * (size_t)len * h->num_nets, cudaMemcpyDeviceToHost,
+          h->stream));
+    }
+    done += len;
+  }
+  return LEV_OK;
+}
+
+int read_states(LevEngine *h, std::vector<NetState> &st) {
+  st.resize(h->num_nets);
+  LEV_TRY_CUDA(cudaMemcpyAsync(st.data(), h->d_st,
+                               sizeof(NetState) * h->num_nets,
+                               cudaMemcpyDeviceToHost, h->stream));
+  LEV_TRY_CUDA(cudaStreamSynchronize(h->stream));
+  return LEV_OK;
+}
+
+int write_state(LevEngine *h, int n, const NetState &s) {
+  LEV_TRY_CUDA(cudaMemcpyAsync(h->d_st + n, &s, sizeof(NetState),
+                               cudaMemcpyHostToDevice, h->stream));
+  LEV_TRY_CUDA(cudaStreamSynchronize(h->stream));
+  return LEV_OK;
+}
+
+int create_impl(LevEngine **out, int num_nets, const int32_t *Ns,
+                const int32_t *mds, const int32_t *rp_cat,
+                const int32_t *col_cat, const uint8_t *d_cat,
+                const float *w_cat, const float *th_cat,
+                const float *thh_cat, const float *om_cat,
+                const LevParams *params, int math_mode) {
+  if (!out) return fail(LEV_ERR_ARG, "out is null");
+  *out = nullptr;
+  if (num_nets < 1) return fail(LEV_ERR_ARG, "num_nets must be >= 1");
+  if (!Ns || !mds || !rp_cat || !th_cat || !thh_cat || !om_cat)
+    return fail(LEV_ERR_ARG, "null array argument");
+  if (math_mode != LEV_MATH_REFERENCE && math_mode != LEV_MATH_ACCURATE)
+    return fail(LEV_ERR_ARG, "math_mode must be 0 (reference) or 1");
+
+  LevEngine *h = new LevEngine();
+  h->num_nets = num_nets;
+  h->math_mode = math_mode;
+  h->h_nets.resize(num_nets);
+  h->net_E.resize(num_nets);
+
+  // ---- validate shapes and lay out the packed arrays ----------------------
+  long long node_off = 0, edge_off = 0, ring_off = 0, rp_off = 0;
+  int tiles = 0;
+  for (int n = 0; n < num_nets; ++n) {
+    const int N = Ns[n], md = mds[n];
+    if (N < 1 || N >= (1 << 24)) {
+      delete h;
+      return fail(LEV_ERR_ARG, "network " + std::to_string(n) +
+                                   ": N must be in [1, 2^24), got " +
+                                   std::to_string(N));
+    }
+    if (md < 0 || md > 255) {
+      delete h;
+      return fail(LEV_ERR_ARG, "network " + std::to_string(n) +
+                                   ": max_delay must be in [0,255] (uint8 "
+                                   "delays), got " + std::to_string(md));
+    }
+    const int32_t *rp = rp_cat + rp_off;
+    if (rp[0] != 0) {
+      delete h;
+      return fail(LEV_ERR_ARG, "network " + std::to_string(n) +
+                                   ": row_ptr[0] must be 0");
+    }
+    for (int i = 0; i < N; ++i) {
+      if (rp[i + 1] < rp[i]) {
+        delete h;
+        return fail(LEV_ERR_ARG, "network " + std::to_string(n) +
+                                     ": row_ptr is decreasing at row " +
+                                     std::to_string(i));
+      }
+    }
+    const long long E = rp[N];
+    NetDesc &d = h->h_nets[n];
+    std::memset(&d, 0, sizeof(d));
+    d.node_off = node_off;
+    d.edge_off = edge_off;
+    d.ring_off = ring_off;
+    d.rp_off = rp_off;
+    d.N = N;
+    d.Np = (N + 31) / 32 * 32;
+    d.bsi = md + 2;
+    d.max_delay = md;
+    d.ntiles = (N + kTile - 1) / kTile;
+    d.part_off = tiles;
+    d.tile_off = tiles;
+    LevParams p;
+    if (params) p = params[n]; else lev_default_params(&p);
+    int rc = check_params(p);
+    if (rc != LEV_OK) {
+      delete h;
+      return rc;
+    }
+    params_to_desc(p, &d);
+    h->net_E[n] = E;
+    node_off += N;
+    edge_off += E;
+    ring_off += (long long)d.bsi * d.Np;
+    rp_off += N + 1;
+    tiles += d.ntiles;
+  }
+  if (edge_off > 0 && (!col_cat || !d_cat || !w_cat)) {
+    delete h;
+    return fail(LEV_ERR_ARG, "null edge array argument");
+  }
+  h->total_nodes = node_off;
+  h->total_edges = edge_off;
+  h->edge_alloc = (edge_off + 3) / 4 * 4 + 4;
+  h->rp_total = rp_off;
+  h->ring_floats = ring_off;
+  h->total_tiles = tiles;
+
+  std::vector<int2> h_tiles(tiles);
+  for (int n = 0; n < num_nets; ++n) {
+    const NetDesc &d = h->h_nets[n];
+    for (int t = 0; t < d.ntiles; ++t)
+      h_tiles[d.tile_off + t] = make_int2(n, t * kTile);
+  }
+
+  // ---- device resources ----------------------------------------------------
+  cudaError_t ce = cudaGetDevice(&h->device);
+  if (ce != cudaSuccess) {
+    delete h;
+    return fail(LEV_ERR_CUDA,
+                std::string("no CUDA device: ") + cudaGetErrorString(ce));
+  }
+  ce = cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking);
+  if (ce != cudaSuccess) {
+    delete h;
+    return fail(LEV_ERR_CUDA, std::string("cudaStreamCreate failed: ") +
+                                  cudaGetErrorString(ce));
+  }
+  int rc = LEV_OK;
+#define LEV_ALLOC(ptr, count)                      \
+  if (rc == LEV_OK) rc = dev_alloc(h, &(ptr), (count));
+  LEV_ALLOC(h->d_nets, (size_t)num_nets);
+  LEV_ALLOC(h->d_st, (size_t)num_nets);
+  LEV_ALLOC(h->d_tiles, (size_t)tiles);
+  LEV_ALLOC(h->d_row_ptr, (size_t)rp_off);
+  LEV_ALLOC(h->d_cd, (size_t)h->edge_alloc);
+  LEV_ALLOC(h->d_w, (size_t)h->edge_alloc);
+  LEV_ALLOC(h->d_theta, (size_t)node_off);
+  LEV_ALLOC(h->d_theta_hat, (size_t)node_off);
+  LEV_ALLOC(h->d_omega, (size_t)node_off);
+  LEV_ALLOC(h->d_omega_hat, (size_t)node_off);
+  LEV_ALLOC(h->d_ring, (size_t)ring_off);
+  LEV_ALLOC(h->d_part, (size_t)tiles);
+  LEV_ALLOC(h->d_rhist, (size_t)h->block_len * num_nets);
+#undef LEV_ALLOC
+  if (rc != LEV_OK) {
+    std::string msg = g_last_error;
+    free_engine(h);
+    return fail(rc, msg);
+  }
+  ce = cudaHostAlloc(reinterpret_cast<void **>(&h->h_rmap),
+                     sizeof(float) * num_nets, cudaHostAllocMapped);
+  if (ce == cudaSuccess)
+    ce = cudaHostGetDevicePointer(reinterpret_cast<void **>(&h->d_rmap),
+                                  h->h_rmap, 0);
+  if (ce != cudaSuccess) {
+    free_engine(h);
+    return fail(LEV_ERR_CUDA, std::string("mapped host buffer: ") +
+                                  cudaGetErrorString(ce));
+  }
+
+  // ---- uploads -------------------------------------------------------------
+  unsigned *d_err = nullptr;
+  uint8_t *d_tmp = nullptr;
+  auto cleanup_fail = [&](int code, const std::string &msg) {
+    if (d_err) cudaFree(d_err);
+    if (d_tmp) cudaFree(d_tmp);
+    free_engine(h);
+    return fail(code, msg);
+  };
+#define LEV_UP(dst, src, bytes)                                            \
+  do {                                                                     \
+    cudaError_t _e = cudaMemcpyAsync((dst), (src), (bytes),                \
+                                     cudaMemcpyHostToDevice, h->stream);   \
+    if (_e != cudaSuccess)                                                 \
+      return cleanup_fail(LEV_ERR_CUDA, std::string("upload failed: ") +   \
+                                            cudaGetErrorString(_e));       \
+  } while (0)
+  LEV_UP(h->d_nets, h->h_nets.data(), sizeof(NetDesc) * num_nets);
+  LEV_UP(h->d_tiles, h_tiles.data(), sizeof(int2) * tiles);
+  LEV_UP(h->d_row_ptr, rp_cat, sizeof(int32_t) * rp_off);
+  LEV_UP(h->d_theta, th_cat, sizeof(float) * node_off);
+  LEV_UP(h->d_theta_hat, thh_cat, sizeof(float) * node_off);
+  LEV_UP(h->d_omega, om_cat, sizeof(float) * node_off);
+  // omega_hat starts as omega (leviathan_kernel.cu:350)
+  LEV_UP(h->d_omega_hat, om_cat, sizeof(float) * node_off);
+  std::vector<NetState> st(num_nets);
+  for (int n = 0; n < num_nets; ++n) {
+    std::memset(&st[n], 0, sizeof(NetState));
+    LevParams p;
+    if (params) p = params[n]; else lev_default_params(&p);
+    st[n].g = p.g;
+  }
+  LEV_UP(h->d_st, st.data(), sizeof(NetState) * num_nets);
+  if (cudaMemsetAsync(h->d_cd, 0, sizeof(uint32_t) * h->edge_alloc,
+                      h->stream) != cudaSuccess ||
+      cudaMemsetAsync(h->d_w, 0, sizeof(float) * h->edge_alloc, h->stream) !=
+          cudaSuccess ||
+      cudaMemsetAsync(h->d_ring, 0, sizeof(float) * std::max<long long>(ring_off, 1),
+                      h->stream) != cudaSuccess)
+    return cleanup_fail(LEV_ERR_CUDA, "memset failed");
+
+  if (edge_off > 0) {
+    LEV_UP(h->d_w, w_cat, sizeof(float) * edge_off);
+    LEV_UP(h->d_cd, col_cat, sizeof(int32_t) * edge_off);
+    if (cudaMalloc(&d_tmp, edge_off) != cudaSuccess ||
+        cudaMalloc(&d_err, sizeof(unsigned)) != cudaSuccess)
+      return cleanup_fail(LEV_ERR_NOMEM, "temporary upload buffer");
+    LEV_UP(d_tmp, d_cat, edge_off);
+    if (cudaMemsetAsync(d_err, 0, sizeof(unsigned), h->stream) != cudaSuccess)
+      return cleanup_fail(LEV_ERR_CUDA, "memset failed");
+    for (int n = 0; n < num_nets; ++n) {
+      const NetDesc &d = h->h_nets[n];
+      const long long E = h->net_E[n];
+      if (E == 0) continue;
+      int blocks = (int)std::min<long long>((E + 255) / 256, 148LL * 32);
+      pack_edges_kernel<<<blocks, 256, 0, h->stream>>>(
+          h->d_cd + d.edge_off, d_tmp + d.edge_off, E, d.N, d.max_delay,
+          d_err);
+    }
+    unsigned herr = 0;
+    cudaError_t e1 = cudaGetLastError();
+    cudaError_t e2 = cudaMemcpyAsync(&herr, d_err, sizeof(unsigned),
+                                     cudaMemcpyDeviceToHost, h->stream);
+    cudaError_t e3 = cudaStreamSynchronize(h->stream);
+    if (e1 != cudaSuccess || e2 != cudaSuccess || e3 != cudaSuccess)
+      return cleanup_fail(LEV_ERR_CUDA,
+                          std::string("edge packing failed: ") +
+                              cudaGetErrorString(e1 != cudaSuccess ? e1
+                                                 : e2 != cudaSuccess ? e2
+                                                                     : e3));
+    if (herr & 1u)
+      return cleanup_fail(LEV_ERR_ARG, "col_idx out of range [0, N)");
+    if (herr & 2u)
+      return cleanup_fail(LEV_ERR_ARG, "delay larger than max_delay");
+    cudaFree(d_tmp);
+    cudaFree(d_err);
+    d_tmp = nullptr;
+    d_err = nullptr;
+  }
+#undef LEV_UP
+  for (int n = 0; n < num_nets; ++n) {
+    int r2 = launch_fill(h, n);
+    if (r2 != LEV_OK) {
+      std::string msg = g_last_error;
+      free_engine(h);
+      return fail(r2, msg);
+    }
+  }
+  ce = cudaStreamSynchronize(h->stream);
+  if (ce != cudaSuccess) {
+    free_engine(h);
+    return fail(LEV_ERR_CUDA,
+                std::string("engine init failed: ") + cudaGetErrorString(ce));
+  }
+  *out = h;
+  return LEV_OK;
+}
+
+}  // namespace
+
+// ===========================================================================
+// lev_* ABI
+// ===========================================================================
+extern "C" {
+
+const char *lev_last_error(void) { return g_last_error.c_str(); }
+
+const char *lev_version(void) { return "leviathan_b200 1.0 (sm_100a)"; }
+
+void lev_default_params(LevParams *p) {
+  if (!p) return;
+  // leviathan_kernel.cu:282-296 and the literal 1.5 at :433
+  p->eta = 0.01f;
+  p->lam = 0.001f;
+  p->gamma = 0.05f;
+  p->alpha_eps = 0.1f;
+  p->kappa_w = 0.01f;
+  p->w_min = 0.0f;
+  p->w_max = 2.0f;
+  p->g = 1.5f;
+  p->r0 = 0.5f;
+  p->beta = 0.01f;
+  p->mu = 0.01f;
+  p->g_rest = 1.5f;
+  p->g_min = 0.1f;
+  p->g_max = 5.0f;
+  p->gain_controller = 1;
+  p->reserved = 0;
+}
+
+int lev_create(LevEngine **out, int32_t N, int32_t max_delay,
+               const int32_t *row_ptr, const int32_t *col_idx,
+               const uint8_t *delays, const float *weights,
+               const float *theta, const float *theta_hat,
+               const float *omega, const LevParams *params,
+               int32_t math_mode) {
+  return create_impl(out, 1, &N, &max_delay, row_ptr, col_idx, delays,
+                     weights, theta, theta_hat, omega, params, math_mode);
+}
+
+int lev_batch_create(LevEngine **out, int32_t num_nets, const int32_t *N,
+                     const int32_t *max_delay, const int32_t *row_ptr_cat,
+                     const int32_t *col_idx_cat, const uint8_t *delays_cat,
+                     const float *weights_cat, const float *theta_cat,
+                     const float *theta_hat_cat, const float *omega_cat,
+                     const LevParams *params, int32_t math_mode) {
+  return create_impl(out, num_nets, N, max_delay, row_ptr_cat, col_idx_cat,
+                     delays_cat, weights_cat, theta_cat, theta_hat_cat,
+                     omega_cat, params, math_mode);
+}
+
+int lev_destroy(LevEngine *h) {
+  if (!h) return LEV_OK;
+  DeviceScope ds(h->device);
+  cudaStreamSynchronize(h->stream);
+  free_engine(h);
+  return LEV_OK;
+}
+
+int lev_num_nets(const LevEngine *h, int32_t *out) {
+  if (!h || !out) return fail(LEV_ERR_ARG, "null argument");
+  *out = h->num_nets;
+  return LEV_OK;
+}
+
+int lev_total_nodes(const LevEngine *h, int64_t *out) {
+  if (!h || !out) return fail(LEV_ERR_ARG, "null argument");
+  *out = h->total_nodes;
+  return LEV_OK;
+}
+
+int lev_total_edges(const LevEngine *h, int64_t *out) {
+  if (!h || !out) return fail(LEV_ERR_ARG, "null argument");
+  *out = h->total_edges;
+  return LEV_OK;
+}
+
+int lev_net_shape(const LevEngine *h, int32_t net, int32_t *N, int64_t *E,
+                  int32_t *max_delay) {
+  if (!h) return fail(LEV_ERR_ARG, "null handle");
+  if (net < 0 || net >= h->num_nets)
+    return fail(LEV_ERR_ARG, "network index out of range");
+  if (N) *N = h->h_nets[net].N;
+  if (E) *E = h->net_E[net];
+  if (max_delay) *max_delay = h->h_nets[net].max_delay;
+  return LEV_OK;
+}
+
+int lev_step(LevEngine *h, float dt, float *r_out) {
+  if (!h) return fail(LEV_ERR_ARG, "null handle");
+  if (!std::isfinite(dt)) return fail(LEV_ERR_ARG, "dt is not finite");
+  DeviceScope ds(h->device);
+  StepArgs a = make_args(h, dt, nullptr, 0, h->d_rmap);
+  int rc = launch_step(h, a);
+  if (rc != LEV_OK) return rc;
+  LEV_TRY_CUDA(cudaStreamSynchronize(h->stream));
+  if (r_out) {
+    const volatile float *src = h->h_rmap;
+    for (int n = 0; n < h->num_nets; ++n) r_out[n] = src[n];
+  }
+  return LEV_OK;
+}
+
+int lev_step_n(LevEngine *h, float dt, int32_t n, float *r_out) {
+  if (!h) return fail(LEV_ERR_ARG, "null handle");
+  if (n < 0) return fail(LEV_ERR_ARG, "n must be >= 0");
+  if (!std::isfinite(dt)) return fail(LEV_ERR_ARG, "dt is not finite");
+  if (n == 0) return LEV_OK;
+  DeviceScope ds(h->device);
+  float *stage = nullptr;
+  if (r_out) {
+    const size_t need = (size_t)n * h->num_nets;
+    if (h->h_rstage_len < need) {
+      if (h->h_rstage) cudaFreeHost(h->h_rstage);
+      h->h_rstage = nullptr;
+      h->h_rstage_len = 0;
+      LEV_TRY_CUDA(cudaMallocHost(reinterpret_cast<void **>(&h->h_rstage),
+                                  sizeof(float) * need));
+      h->h_rstage_len = need;
+    }
+    stage = h->h_rstage;
+  }
+  int rc = enqueue_steps(h, dt, n, stage);
+  if (rc != LEV_OK) return rc;
+  LEV_TRY_CUDA(cudaStreamSynchronize(h->stream));
+  if (r_out)
+    std::memcpy(r_out, stage, sizeof(float) * (size_t)n * h->num_nets);
+  return LEV_OK;
+}
+
+int lev_step_n_async(LevEngine *h, float dt, int32_t n) {
+  if (!h) return fail(LEV_ERR_ARG, "null handle");
+  if (n < 0) return fail(LEV_ERR_ARG, "n must be >= 0");
+  if (!std::isfinite(dt)) return fail(LEV_ERR_ARG, "dt is not finite");
+  DeviceScope ds(h->device);
+  return enqueue_steps(h, dt, n, nullptr);
+}
+
+int lev_sync(LevEngine *h) {
+  if (!h) return fail(LEV_ERR_ARG, "null handle");
+  DeviceScope ds(h->device);
+  LEV_TRY_CUDA(cudaStreamSynchronize(h->stream));
+  return LEV_OK;
+}
+
+int lev_get_stream(LevEngine *h, void **stream) {
+  if (!h || !stream) return fail(LEV_ERR_ARG, "null argument");
+  *stream = reinterpret_cast<void *>(h->stream);
+  return LEV_OK;
+}
+
+static int copy_nodes(LevEngine *h, float *dst_host, const float *src_dev,
+                      long long off, long long count) {
+  LEV_TRY_CUDA(cudaMemcpyAsync(dst_host, src_dev + off, sizeof(float) * count,
+                               cudaMemcpyDeviceToHost, h->stream));
+  LEV_TRY_CUDA(cudaStreamSynchronize(h->stream));
+  return LEV_OK;
+}
+
+static int upload_nodes(LevEngine *h, float *dst_dev, const float *src_host,
+                        long long off, long long count) {
+  LEV_TRY_CUDA(cudaMemcpyAsync(dst_dev + off, src_host, sizeof(float) * count,
+                               cudaMemcpyHostToDevice, h->stream));
+  return LEV_OK;
+}
+
+int lev_get_theta(LevEngine *h, float *theta_out) {
+  if (!h || !theta_out) return fail(LEV_ERR_ARG, "null argument");
+  DeviceScope ds(h->device);
+  return copy_nodes(h, theta_out, h->d_theta, 0, h->total_nodes);
+}
+
+int lev_get_theta_net(LevEngine *h, int32_t net, float *theta_out) {
+  if (!h || !theta_out) return fail(LEV_ERR_ARG, "null argument");
+  if (net < 0 || net >= h->num_nets)
+    return fail(LEV_ERR_ARG, "network index out of range");
+  DeviceScope ds(h->device);
+  const NetDesc &d = h->h_nets[net];
+  return copy_nodes(h, theta_out, h->d_theta, d.node_off, d.N);
+}
+
+int lev_set_theta(LevEngine *h, const float *theta_in) {
+  if (!h || !theta_in) return fail(LEV_ERR_ARG, "null argument");
+  DeviceScope ds(h->device);
+  int rc = upload_nodes(h, h->d_theta, theta_in, 0, h->total_nodes);
+  for (int n = 0; n < h->num_nets && rc == LEV_OK; ++n) rc = launch_fill(h, n);
+  if (rc != LEV_OK) return rc;
+  LEV_TRY_CUDA(cudaStreamSynchronize(h->stream));
+  return LEV_OK;
+}
+
+int lev_set_theta_net(LevEngine *h, int32_t net, const float *theta_in) {
+  if (!h || !theta_in) return fail(LEV_ERR_ARG, "null argument");
+  if (net < 0 || net >= h->num_nets)
+    return fail(LEV_ERR_ARG, "network index out of range");
+  DeviceScope ds(h->device);
+  const NetDesc &d = h->h_nets[net];
+  int rc = upload_nodes(h, h->d_theta, theta_in, d.node_off, d.N);
+  if (rc == LEV_OK) rc = launch_fill(h, net);
+  if (rc != LEV_OK) return rc;
+  LEV_TRY_CUDA(cudaStreamSynchronize(h->stream));
+  return LEV_OK;
+}
+
+int lev_get_weights(LevEngine *h, float *w_out) {
+  if (!h || (!w_out && h->total_edges > 0))
+    return fail(LEV_ERR_ARG, "null argument");
+  DeviceScope ds(h->device);
+  if (h->total_edges == 0) return LEV_OK;
+  return copy_nodes(h, w_out, h->d_w, 0, h->total_edges);
+}
+
+int lev_reset_weights(LevEngine *h, const float *w_in) {
+  if (!h || (!w_in && h->total_edges > 0))
+    return fail(LEV_ERR_ARG, "null argument");
+  DeviceScope ds(h->device);
+  if (h->total_edges == 0) return LEV_OK;
+  int rc = upload_nodes(h, h->d_w, w_in, 0, h->total_edges);
+  if (rc != LEV_OK) return rc;
+  LEV_TRY_CUDA(cudaStreamSynchronize(h->stream));
+  return LEV_OK;
+}
+
+int lev_get_predictor(LevEngine *h, float *theta_hat_out,
+                      float *omega_hat_out) {
+  if (!h) return fail(LEV_ERR_ARG, "null handle");
+  DeviceScope ds(h->device);
+  int rc = LEV_OK;
+  if (theta_hat_out)
+    rc = copy_nodes(h, theta_hat_out, h->d_theta_hat, 0, h->total_nodes);
+  if (rc == LEV_OK && omega_hat_out)
+    rc = copy_nodes(h, omega_hat_out, h->d_omega_hat, 0, h->total_nodes);
+  return rc;
+}
+
+int lev_set_predictor(LevEngine *h, const float *theta_hat_in,
+                      const float *omega_hat_in) {
+  if (!h) return fail(LEV_ERR_ARG, "null handle");
+  DeviceScope ds(h->device);
+  int rc = LEV_OK;
+  if (theta_hat_in)
+    rc = upload_nodes(h, h->d_theta_hat, theta_hat_in, 0, h->total_nodes);
+  if (rc == LEV_OK && omega_hat_in)
+    rc = upload_nodes(h, h->d_omega_hat, omega_hat_in, 0, h->total_nodes);
+  if (rc != LEV_OK) return rc;
+  LEV_TRY_CUDA(cudaStreamSynchronize(h->stream));
+  return LEV_OK;
+}
+
+int lev_get_omega(LevEngine *h, float *omega_out) {
+  if (!h || !omega_out) return fail(LEV_ERR_ARG, "null argument");
+  DeviceScope ds(h->device);
+  return copy_nodes(h, omega_out, h->d_omega, 0, h->total_nodes);
+}
+
+int lev_set_omega(LevEngine *h, const float *omega_in) {
+  if (!h || !omega_in) return fail(LEV_ERR_ARG, "null argument");
+  DeviceScope ds(h->device);
+  int rc = upload_nodes(h, h->d_omega, omega_in, 0, h->total_nodes);
+  if (rc != LEV_OK) return rc;
+  LEV_TRY_CUDA(cudaStreamSynchronize(h->stream));
+  return LEV_OK;
+}
+
+int lev_get_ring(LevEngine *h, int32_t net, float *ring_out,
+                 int32_t *buf_idx) {
+  if (!h || !ring_out) return fail(LEV_ERR_ARG, "null argument");
+  if (net < 0 || net >= h->num_nets)
+    return fail(LEV_ERR_ARG, "network index out of range");
+  DeviceScope ds(h->device);
+  std::vector<NetState> st;
+  int rc = read_states(h, st);
+  if (rc != LEV_OK) return rc;
+  const NetDesc &d = h->h_nets[net];
+  std::vector<float> ri((size_t)d.bsi * d.Np);
+  LEV_TRY_CUDA(cudaMemcpyAsync(ri.data(), h->d_ring + d.ring_off,
+                               sizeof(float) * ri.size(),
+                               cudaMemcpyDeviceToHost, h->stream));
+  LEV_TRY_CUDA(cudaStreamSynchronize(h->stream));
+  const int bs = d.max_delay + 1;
+  const int cur = st[net].cur, rb = st[net].rbuf;
+  for (int m = 0; m <= d.max_delay; ++m) {
+    const int si = ((cur - m) % d.bsi + d.bsi) % d.bsi;
+    const int sr = ((rb - m) % bs + bs) % bs;
+    const float *src = ri.data() + (size_t)si * d.Np;
+    for (int j = 0; j < d.N; ++j) ring_out[(size_t)j * bs + sr] = src[j];
+  }
+  if (buf_idx) *buf_idx = rb;
+  return LEV_OK;
+}
+
+int lev_set_ring(LevEngine *h, int32_t net, const float *ring_in,
+                 int32_t buf_idx) {
+  if (!h || !ring_in) return fail(LEV_ERR_ARG, "null argument");
+  if (net < 0 || net >= h->num_nets)
+    return fail(LEV_ERR_ARG, "network index out of range");
+  const NetDesc &d = h->h_nets[net];
+  const int bs = d.max_delay + 1;
+  if (buf_idx < 0 || buf_idx >= bs)
+    return fail(LEV_ERR_ARG, "buf_idx out of range [0, max_delay]");
+  DeviceScope ds(h->device);
+  std::vector<NetState> st;
+  int rc = read_states(h, st);
+  if (rc != LEV_OK) return rc;
+  std::vector<float> ri((size_t)d.bsi * d.Np, 0.0f);
+  const int cur = st[net].cur;
+  for (int m = 0; m <= d.max_delay; ++m) {
+    const int si = ((cur - m) % d.bsi + d.bsi) % d.bsi;
+    const int sr = ((buf_idx - m) % bs + bs) % bs;
+    float *dst = ri.data() + (size_t)si * d.Np;
+    for (int j = 0; j < d.N; ++j) dst[j] = ring_in[(size_t)j * bs + sr];
+  }
+  LEV_TRY_CUDA(cudaMemcpyAsync(h->d_ring + d.ring_off, ri.data(),
+                               sizeof(float) * ri.size(),
+                               cudaMemcpyHostToDevice, h->stream));
+  NetState s = st[net];
+  s.rbuf = buf_idx;
+  return write_state(h, net, s);
+}
+
+int lev_get_step_count(LevEngine *h, int32_t net, int64_t *t) {
+  if (!h || !t) return fail(LEV_ERR_ARG, "null argument");
+  if (net < 0 || net >= h->num_nets)
+    return fail(LEV_ERR_ARG, "network index out of range");
+  DeviceScope ds(h->device);
+  std::vector<NetState> st;
+  int rc = read_states(h, st);
+  if (rc != LEV_OK) return rc;
+  *t = st[net].t;
+  return LEV_OK;
+}
+
+int lev_set_gain(LevEngine *h, int32_t net, float g) {
+  if (!h) return fail(LEV_ERR_ARG, "null handle");
+  if (net < -1 || net >= h->num_nets)
+    return fail(LEV_ERR_ARG, "network index out of range");
+  DeviceScope ds(h->device);
+  std::vector<NetState> st;
+  int rc = read_states(h, st);
+  if (rc != LEV_OK) return rc;
+  for (int n = 0; n < h->num_nets; ++n) {
+    if (net >= 0 && n != net) continue;
+    st[n].g = g;
+  }
+  LEV_TRY_CUDA(cudaMemcpyAsync(h->d_st, st.data(),
+                               sizeof(NetState) * h->num_nets,
+                               cudaMemcpyHostToDevice, h->stream));
+  LEV_TRY_CUDA(cudaStreamSynchronize(h->stream));
+  return LEV_OK;
+}
+
+int lev_get_gain(LevEngine *h, int32_t net, float *g) {
+  if (!h || !g) return fail(LEV_ERR_ARG, "null argument");
+  if (net < 0 || net >= h->num_nets)
+    return fail(LEV_ERR_ARG, "network index out of range");
+  DeviceScope ds(h->device);
+  std::vector<NetState> st;
+  int rc = read_states(h, st);
+  if (rc != LEV_OK) return rc;
+  *g = st[net].g;
+  return LEV_OK;
+}
+
+int lev_get_r(LevEngine *h, int32_t net, float *r) {
+  if (!h || !r) return fail(LEV_ERR_ARG, "null argument");
+  if (net < 0 || net >= h->num_nets)
+    return fail(LEV_ERR_ARG, "network index out of range");
+  DeviceScope ds(h->device);
+  std::vector<NetState> st;
+  int rc = read_states(h, st);
+  if (rc != LEV_OK) return rc;
+  *r = st[net].r;
+  return LEV_OK;
+}
+
+int lev_set_gain_controller(LevEngine *h, int32_t net, int32_t enabled) {
+  if (!h) return fail(LEV_ERR_ARG, "null handle");
+  if (net < -1 || net >= h->num_nets)
+    return fail(LEV_ERR_ARG, "network index out of range");
+  DeviceScope ds(h->device);
+  for (int n = 0; n < h->num_nets; ++n) {
+    if (net >= 0 && n != net) continue;
+    h->h_nets[n].ctrl = enabled ? 1 : 0;
+  }
+  LEV_TRY_CUDA(cudaMemcpyAsync(h->d_nets, h->h_nets.data(),
+                               sizeof(NetDesc) * h->num_nets,
+                               cudaMemcpyHostToDevice, h->stream));
+  LEV_TRY_CUDA(cudaStreamSynchronize(h->stream));
+  return LEV_OK;
+}
+
+int lev_set_params(LevEngine *h, int32_t net, const LevParams *p) {
+  if (!h || !p) return fail(LEV_ERR_ARG, "null argument");
+  if (net < -1 || net >= h->num_nets)
+    return fail(LEV_ERR_ARG, "network index out of range");
+  int rc = check_params(*p);
+  if (rc != LEV_OK) return rc;
+  DeviceScope ds(h->device);
+  std::vector<NetState> st;
+  rc = read_states(h, st);
+  if (rc != LEV_OK) return rc;
+  for (int n = 0; n < h->num_nets; ++n) {
+    if (net >= 0 && n != net) continue;
+    params_to_desc(*p, &h->h_nets[n]);
+    st[n].g = p->g;
+  }
+  LEV_TRY_CUDA(cudaMemcpyAsync(h->d_nets, h->h_nets.data(),
+                               sizeof(NetDesc) * h->num_nets,
+                               cudaMemcpyHostToDevice, h->stream));
+  LEV_TRY_CUDA(cudaMemcpyAsync(h->d_st, st.data(),
+                               sizeof(NetState) * h->num_nets,
+                               cudaMemcpyHostToDevice, h->stream));
+  LEV_TRY_CUDA(cudaStreamSynchronize(h->stream));
+  return LEV_OK;
+}
+
+int lev_get_params(LevEngine *h, int32_t net, LevParams *p) {
+  if (!h || !p) return fail(LEV_ERR_ARG, "null argument");
+  if (net < 0 || net >= h->num_nets)
+    return fail(LEV_ERR_ARG, "network index out of range");
+  float g = 0.0f;
+  int rc = lev_get_gain(h, net, &g);
+  if (rc != LEV_OK) return rc;
+  desc_to_params(h->h_nets[net], g, p);
+  return LEV_OK;
+}
+
+int lev_set_math_mode(LevEngine *h, int32_t math_mode) {
+  if (!h) return fail(LEV_ERR_ARG, "null handle");
+  if (math_mode != LEV_MATH_REFERENCE && math_mode != LEV_MATH_ACCURATE)
+    return fail(LEV_ERR_ARG, "math_mode must be 0 (reference) or 1");
+  h->math_mode = math_mode;
+  return LEV_OK;
+}
+
+int lev_get_vram_usage(const LevEngine *h, size_t *bytes) {
+  if (!h || !bytes) return fail(LEV_ERR_ARG, "null argument");
+  *bytes = h->vram;
+  return LEV_OK;
+}
+
+// ===========================================================================
+// Reference ABI (leviathan_kernel.cu:21-499)
+// ===========================================================================
+static void report(const char *fn) {
+  std::fprintf(stderr, "[leviathan_b200] %s: %s\n", fn, g_last_error.c_str());
+}
+
+LeviathanHandle *leviathan_init(int N, int max_delay, int *h_row_ptr,
+                                int *h_col_idx, uint8_t *h_delays,
+                                float *h_weights, float *h_theta,
+                                float *h_theta_hat, float *h_omega) {
+  LevEngine *e = nullptr;
+  if (lev_create(&e, N, max_delay, h_row_ptr, h_col_idx, h_delays, h_weights,
+                 h_theta, h_theta_hat, h_omega, nullptr,
+                 LEV_MATH_REFERENCE) != LEV_OK) {
+    report("leviathan_init");
+    return nullptr;
+  }
+  LeviathanHandle *h = new LeviathanHandle();
+  h->eng = e;
+  return h;
+}
+
+float leviathan_step(LeviathanHandle *handle, float dt) {
+  if (!handle) {
+    fail(LEV_ERR_ARG, "null handle");
+    return std::numeric_limits<float>::quiet_NaN();
+  }
+  float r = 0.0f;
+  if (lev_step(handle->eng, dt, &r) != LEV_OK) {
+    report("leviathan_step");
+    return std::numeric_limits<float>::quiet_NaN();
+  }
+  return r;
+}
+
+void leviathan_get_theta(LeviathanHandle *handle, float *h_theta) {
+  if (!handle || lev_get_theta(handle->eng, h_theta) != LEV_OK)
+    report("leviathan_get_theta");
+}
+
+void leviathan_set_theta(LeviathanHandle *handle, float *h_theta) {
+  if (!handle || lev_set_theta(handle->eng, h_theta) != LEV_OK)
+    report("leviathan_set_theta");
+}
+
+void leviathan_free(LeviathanHandle *handle) {
+  if (!handle) return;
+  lev_destroy(handle->eng);
+  delete handle;
+}
+
+void leviathan_set_gain(LeviathanHandle *handle, float g) {
+  if (!handle || lev_set_gain(handle->eng, 0, g) != LEV_OK)
+    report("leviathan_set_gain");
+}
+
+float leviathan_get_gain(LeviathanHandle *handle) {
+  float g = std::numeric_limits<float>::quiet_NaN();
+  if (!handle || lev_get_gain(handle->eng, 0, &g) != LEV_OK)
+    report("leviathan_get_gain");
+  return g;
+}
+
+void leviathan_set_gain_controller(LeviathanHandle *handle, bool enabled) {
+  if (!handle ||
+      lev_set_gain_controller(handle->eng, 0, enabled ? 1 : 0) != LEV_OK)
+    report("leviathan_set_gain_controller");
+}
+
+size_t leviathan_get_vram_usage(LeviathanHandle *handle) {
+  size_t b = 0;
+  if (!handle || lev_get_vram_usage(handle->eng, &b) != LEV_OK)
+    report("leviathan_get_vram_usage");
+  return b;
+}
+
+void leviathan_reset_weights(LeviathanHandle *handle, float *h_weights) {
+  if (!handle || lev_reset_weights(handle->eng, h_weights) != LEV_OK)
+    report("leviathan_reset_weights");
+}
+
+LevEngine *leviathan_engine(LeviathanHandle *handle) {
+  return handle ? handle->eng : nullptr;
+}
+
+}  // extern "C"

@@ -1,0 +1,264 @@
+"""Parity of the B200 engine (CUDA, through the C ABI) with the reference
+engine and the FP64 oracle.  Needs a CUDA device.
+
+Tolerances (FP32, stated here and asserted):
+* against the reference engine, same inputs, reference math mode, <= 200
+  steps: phases within 1e-4 rad (circular distance), weights within 1e-5,
+  r within 1e-5 -- and the fraction of bit-identical values is asserted
+  separately where the arithmetic is identical;
+* against the FP64 oracle over 200 steps: wrapped phase error <= 1e-4 rad in
+  accurate math mode;
+* integer / index work (ring slots, buf_idx, step count) is exact.
+"""
+
+import numpy as np
+import pytest
+
+from conftest import (LevAdapter, OracleAdapter, golden_cases, has_gpu,
+                      load_golden, network_from_golden, record_from_golden)
+from leviathan_v1_b200 import BatchEngine, LeviathanEngine
+from leviathan_v1_b200.graphs import make_network
+from make_golden import decode_actions, replay
+from oracle64 import OracleEngine, circular_distance
+
+pytestmark = pytest.mark.gpu
+
+DT = 0.05
+REF_TOL = dict(r=1e-5, theta=1e-4, w=1e-5, hat=1e-4)
+
+
+@pytest.fixture(scope="module", autouse=True)
+def _need_gpu():
+    if not has_gpu():
+        pytest.fail("GPU tests need a CUDA device")
+
+
+def _cmp(name, got, want, tol, nan_equal=True):
+    got = np.asarray(got, np.float64)
+    want = np.asarray(want, np.float64)
+    fin = np.isfinite(want)
+    if nan_equal:
+        assert np.array_equal(np.isfinite(got), fin), f"{name}: NaN pattern"
+    if name.startswith(("theta@", "ring@")):
+        err = circular_distance(got[fin], want[fin]).max(initial=0)
+    else:
+        err = np.abs(got[fin] - want[fin]).max(initial=0)
+    assert err <= tol, f"{name}: max error {err} > {tol}"
+    return err
+
+
+# ---------------------------------------------------------------------------
+# Reference golden vectors (the reference engine's own outputs)
+# ---------------------------------------------------------------------------
+@pytest.mark.skipif(not golden_cases(), reason="golden vectors not generated")
+@pytest.mark.parametrize("case", golden_cases() or ["none"])
+def test_engine_matches_reference_golden(case):
+    z = load_golden(case)
+    net = network_from_golden(z)
+    eng = LevAdapter(net, "reference")
+    rs, snaps = replay(eng, decode_actions(z), record_from_golden(z), dt=float(z["dt"]))
+    eng.close()
+    ref_r = z["r"]
+    horizon = min(200, rs.size)
+    _cmp("r", rs[:horizon], ref_r[:horizon], REF_TOL["r"])
+    for key, got in snaps.items():
+        name, t = key.split("@")
+        if int(t) > 200:
+            continue
+        want = z[key]
+        if name == "buf_idx":
+            assert int(got) == int(want), key
+        elif name in ("theta", "ring"):
+            _cmp(key, got, want, REF_TOL["theta"])
+        elif name == "weights":
+            _cmp(key, got, want, REF_TOL["w"])
+        elif name in ("theta_hat", "omega_hat"):
+            _cmp(key, got, want, REF_TOL["hat"])
+        elif name == "g":
+            assert abs(float(got) - float(want)) <= 1e-5, key
+
+
+@pytest.mark.skipif(not golden_cases(), reason="golden vectors not generated")
+@pytest.mark.parametrize("case", golden_cases() or ["none"])
+def test_engine_bit_identical_to_reference_golden(case):
+    """Reference math mode reproduces the reference engine bit for bit
+    (same expressions, same intrinsic, same summation order)."""
+    z = load_golden(case)
+    net = network_from_golden(z)
+    eng = LevAdapter(net, "reference")
+    rs, snaps = replay(eng, decode_actions(z), record_from_golden(z), dt=float(z["dt"]))
+    eng.close()
+    np.testing.assert_array_equal(rs, z["r"])
+    for key, got in snaps.items():
+        np.testing.assert_array_equal(np.asarray(got), z[key], err_msg=key)
+
+
+# ---------------------------------------------------------------------------
+# Live reference engine (oracle/_ref) on larger inputs
+# ---------------------------------------------------------------------------
+def _ref_engine(net, flavor="sm100a"):
+    from refengine import RefEngine, available
+
+    if not available(flavor):
+        pytest.fail("oracle/_ref/ reference build missing (run make -C oracle)")
+    return RefEngine(*net.engine_args(), flavor=flavor)
+
+
+@pytest.mark.parametrize("N,k,md,steps", [(20_000, 16, 30, 60), (100_000, 32, 64, 20),
+                                          (1_000_000, 32, 64, 5)])
+def test_engine_matches_live_reference(N, k, md, steps):
+    net = make_network(N, k, 0.1, md, seed=N)
+    ref = _ref_engine(net)
+    eng = LeviathanEngine(*net.engine_args())
+    r_ref = ref.run(DT, steps)
+    r_eng = np.array([eng.step(DT) for _ in range(steps)], np.float32)
+    s = ref.state()
+    _cmp("r", r_eng, r_ref, REF_TOL["r"])
+    _cmp("theta@", eng.get_theta(), s["theta"], REF_TOL["theta"])
+    _cmp("weights", eng.get_weights(), s["weights"], REF_TOL["w"])
+    ring, bi = eng.get_ring(0)
+    assert bi == s["buf_idx"] == steps % (md + 1)
+    _cmp("ring@", ring, s["ring"], REF_TOL["theta"])
+    assert abs(eng.get_gain() - s["g"]) <= 1e-5
+    same = np.mean(eng.get_theta() == s["theta"])
+    assert same > 0.999, f"only {same:.4%} of phases bit-identical"
+    ref.close()
+    eng.close()
+
+
+def test_stock_reference_build_agrees():
+    """The reference's stock arch list (PTX JIT on B200) runs and agrees."""
+    net = make_network(5000, 16, 0.1, 20, seed=9)
+    a = _ref_engine(net, "sm100a")
+    b = _ref_engine(net, "stock")
+    ra, rb = a.run(DT, 30), b.run(DT, 30)
+    _cmp("r", ra, rb, REF_TOL["r"])
+    a.close()
+    b.close()
+
+
+# ---------------------------------------------------------------------------
+# FP64 oracle
+# ---------------------------------------------------------------------------
+@pytest.mark.parametrize("mode,tol", [("accurate", 1e-4), ("reference", 2e-3)])
+def test_error_against_fp64_oracle(mode, tol):
+    net = make_network(1000, 20, 0.1, 50, seed=0, generator="networkx")
+    eng = LeviathanEngine(*net.engine_args(), math_mode=mode)
+    o = OracleEngine(*net.engine_args())
+    r_eng = eng.step_n(DT, 200)
+    r_o = o.run(DT, 200)
+    err = circular_distance(eng.get_theta(), o.theta).max()
+    assert err <= tol, f"{mode}: wrapped phase error {err}"
+    assert np.abs(r_eng - r_o).max() <= 10 * tol
+    eng.close()
+
+
+# ---------------------------------------------------------------------------
+# Engine properties
+# ---------------------------------------------------------------------------
+def test_step_n_equals_repeated_step():
+    net = make_network(3000, 12, 0.1, 25, seed=4)
+    a = LeviathanEngine(*net.engine_args())
+    b = LeviathanEngine(*net.engine_args())
+    ra = np.array([a.step(DT) for _ in range(300)], np.float32)
+    rb = np.concatenate([b.step_n(DT, 7), b.step_n(DT, 256), b.step_n(DT, 37)])
+    np.testing.assert_array_equal(ra, rb)
+    np.testing.assert_array_equal(a.get_theta(), b.get_theta())
+    np.testing.assert_array_equal(a.get_weights(), b.get_weights())
+    assert a.step_count() == b.step_count() == 300
+
+
+def test_batch_equals_individual_engines():
+    nets = [make_network(n, k, 0.1, md, seed=s, delay_lo=min(1, md))
+            for n, k, md, s in [(700, 8, 10, 1), (2500, 20, 50, 2), (256, 4, 3, 3),
+                                (1000, 16, 0, 4), (4097, 32, 64, 5)]]
+    params = [dict(g=0.5 * i, gain_controller=i % 2) for i in range(len(nets))]
+    be = BatchEngine([n.as_dict() for n in nets], params=params)
+    rb = be.step_n(DT, 120)
+    for i, n in enumerate(nets):
+        e = LeviathanEngine(*n.engine_args(), params=params[i])
+        ri = e.step_n(DT, 120)
+        np.testing.assert_array_equal(rb[:, i], ri)
+        np.testing.assert_array_equal(be.get_theta(i), e.get_theta())
+        e.close()
+    be.close()
+
+
+def test_checkpoint_round_trip_is_exact():
+    net = make_network(5000, 16, 0.1, 40, seed=8)
+    e = LeviathanEngine(*net.engine_args())
+    e.step_n(DT, 25)
+    st = e.get_state()
+    r1 = e.step_n(DT, 60)
+    th1 = e.get_theta()
+    e.set_state(st)
+    r2 = e.step_n(DT, 60)
+    np.testing.assert_array_equal(r1, r2)
+    np.testing.assert_array_equal(th1, e.get_theta())
+    e.close()
+
+
+def test_set_theta_refills_ring_and_resets_history():
+    net = make_network(2000, 10, 0.1, 15, seed=2)
+    e = LeviathanEngine(*net.engine_args())
+    e.step_n(DT, 33)
+    th = np.linspace(0, 6.0, 2000).astype(np.float32)
+    e.set_theta(th)
+    ring, bi = e.get_ring()
+    assert bi == 33 % 16
+    np.testing.assert_array_equal(ring, np.repeat(th[:, None], 16, axis=1))
+    with pytest.raises(RuntimeError, match="size mismatch"):
+        e.set_theta(th[:10])
+    e.close()
+
+
+def test_invariants_at_scale():
+    net = make_network(1_000_000, 32, 0.1, 64, seed=0)
+    e = LeviathanEngine(*net.engine_args())
+    r = e.step_n(DT, 50)
+    th = e.get_theta()
+    w = e.get_weights()
+    assert np.all(np.isfinite(th)) and th.min() >= 0 and th.max() < 2 * np.pi + 1e-5
+    assert np.all((r >= 0) & (r <= 1))
+    assert w.min() >= 0 and w.max() <= 2
+    assert e.step_count() == 50
+    e.close()
+
+
+def test_invalid_topology_rejected_on_device():
+    net = make_network(500, 8, 0.1, 10, seed=1)
+    col = net.col_idx.copy()
+    col[17] = 500
+    with pytest.raises(ValueError, match="col_idx"):
+        LeviathanEngine(net.N, 10, net.row_ptr, col, net.delays, net.weights,
+                        net.theta, net.theta_hat, net.omega)
+    d = net.delays.copy()
+    d[3] = 11
+    with pytest.raises(ValueError, match="delay"):
+        LeviathanEngine(net.N, 10, net.row_ptr, net.col_idx, d, net.weights,
+                        net.theta, net.theta_hat, net.omega)
+
+
+def test_reference_abi_layer():
+    """The reference's C ABI on this library behaves like the Python class."""
+    import ctypes as C
+
+    from leviathan_v1_b200 import _lib
+
+    lib = _lib.load()
+    net = make_network(800, 8, 0.1, 12, seed=6)
+    arrs = [np.ascontiguousarray(a) for a in net.engine_args()[2:]]
+    P = lambda a: C.c_void_p(a.ctypes.data)
+    h = lib.leviathan_init(net.N, net.max_delay, *[P(a) for a in arrs])
+    assert h
+    e = LeviathanEngine(*net.engine_args())
+    for _ in range(20):
+        assert lib.leviathan_step(h, C.c_float(DT)) == np.float32(e.step(DT))
+    th = np.empty(net.N, np.float32)
+    lib.leviathan_get_theta(h, P(th))
+    np.testing.assert_array_equal(th, e.get_theta())
+    lib.leviathan_set_gain(h, C.c_float(2.0))
+    assert lib.leviathan_get_gain(h) == np.float32(2.0)
+    assert lib.leviathan_get_vram_usage(h) > 0
+    lib.leviathan_free(h)
+    e.close()
