@@ -216,6 +216,14 @@ int lev_set_math_mode(LevEngine *h, int32_t math_mode);
  * bytes actually allocated. */
 int lev_get_vram_usage(const LevEngine *h, size_t *bytes);
 
+/* Self-test of the phase wraps (no reference counterpart; checks this
+ * library's division-free evaluation of the wraps of
+ * leviathan_kernel.cu:105,146,188).  Runs, on the current device, both
+ * wraps for all 2^32 float inputs against the same expressions with IEEE
+ * division; *mismatch_pm / *mismatch_02 receive the number of inputs whose
+ * results differ in any bit (0 expected). */
+int lev_selftest_wraps(uint64_t *mismatch_pm, uint64_t *mismatch_02);
+
 /* ------------------------------------------------------------------------ */
 /* Reference C ABI (leviathan_kernel.cu:21-499), same symbols and signatures */
 /* ------------------------------------------------------------------------ */

@@ -99,6 +99,7 @@ PROTOTYPES = {
     "lev_get_params": (C.c_int, [_P, _i32, C.POINTER(LevParams)]),
     "lev_set_math_mode": (C.c_int, [_P, _i32]),
     "lev_get_vram_usage": (C.c_int, [_P, C.POINTER(C.c_size_t)]),
+    "lev_selftest_wraps": (C.c_int, [C.POINTER(C.c_uint64), C.POINTER(C.c_uint64)]),
     # reference ABI (leviathan_kernel.cu:21-499)
     "leviathan_init": (_P, [C.c_int, C.c_int, _P, _P, _P, _P, _P, _P, _P]),
     "leviathan_step": (_f32, [_P, _f32]),

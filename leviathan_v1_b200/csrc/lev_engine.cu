@@ -67,11 +67,13 @@ struct LevEngine {
   int num_nets = 0;
   long long total_nodes = 0;
   long long total_edges = 0;   // sum of E
-  long long edge_alloc = 0;    // padded edge allocation (multiple of 4, +4)
+  long long num_slices = 0;    // SELL-32 slices over all networks
+  long long sl_total = 0;      // SELL-32 entries (multiple of 32)
   long long rp_total = 0;
   long long ring_floats = 0;
   int total_tiles = 0;
   int math_mode = LEV_MATH_REFERENCE;
+  int sweep = 0;  // direction of the next step's walk over the tiles
   size_t vram = 0;
 
   std::vector<NetDesc> h_nets;
@@ -81,8 +83,10 @@ struct LevEngine {
   NetState *d_st = nullptr;
   int2 *d_tiles = nullptr;
   int *d_row_ptr = nullptr;
-  uint32_t *d_cd = nullptr;
-  float *d_w = nullptr;
+  long long *d_sl_off = nullptr;
+  int *d_sl_len = nullptr;
+  uint32_t *d_sl_cd = nullptr;
+  float *d_sl_w = nullptr;
   float *d_theta = nullptr;
   float *d_theta_hat = nullptr;
   float *d_omega = nullptr;
@@ -134,8 +138,10 @@ void free_engine(LevEngine *h) {
   cudaFree(h->d_st);
   cudaFree(h->d_tiles);
   cudaFree(h->d_row_ptr);
-  cudaFree(h->d_cd);
-  cudaFree(h->d_w);
+  cudaFree(h->d_sl_off);
+  cudaFree(h->d_sl_len);
+  cudaFree(h->d_sl_cd);
+  cudaFree(h->d_sl_w);
   cudaFree(h->d_theta);
   cudaFree(h->d_theta_hat);
   cudaFree(h->d_omega);
@@ -213,8 +219,10 @@ StepArgs make_args(LevEngine *h, float dt, float *r_hist, int r_cap,
   a.st = h->d_st;
   a.tiles = h->d_tiles;
   a.row_ptr = h->d_row_ptr;
-  a.cd = h->d_cd;
-  a.w = h->d_w;
+  a.sl_off = h->d_sl_off;
+  a.sl_len = h->d_sl_len;
+  a.sl_cd = h->d_sl_cd;
+  a.sl_w = h->d_sl_w;
   a.theta = h->d_theta;
   a.theta_hat = h->d_theta_hat;
   a.omega = h->d_omega;
@@ -226,10 +234,32 @@ StepArgs make_args(LevEngine *h, float dt, float *r_hist, int r_cap,
   a.r_cap = r_cap;
   a.num_nets = h->num_nets;
   a.dt = dt;
+  a.reverse = 0;
   return a;
 }
 
-int launch_step(LevEngine *h, const StepArgs &a) {
+// The step kernel keeps almost nothing in shared memory; prefer the largest
+// L1 carve-out so ring gathers reuse lines across a tile's rows.
+int prepare_step_kernels() {
+  LEV_TRY_CUDA(cudaFuncSetAttribute(step_kernel<0>,
+                                    cudaFuncAttributePreferredSharedMemoryCarveout,
+                                    (int)cudaSharedmemCarveoutMaxL1));
+  LEV_TRY_CUDA(cudaFuncSetAttribute(step_kernel<1>,
+                                    cudaFuncAttributePreferredSharedMemoryCarveout,
+                                    (int)cudaSharedmemCarveoutMaxL1));
+  return LEV_OK;
+}
+
+// Launches one step.  Successive steps alternate the direction in which
+// CTAs walk the tile list, so the ring lines touched at the end of one step
+// are the first touched by the next while they are still in L2; results do
+// not depend on the direction.
+#ifndef LEV_SWEEP_ALTERNATE
+#define LEV_SWEEP_ALTERNATE 1
+#endif
+int launch_step(LevEngine *h, StepArgs a) {
+  a.reverse = LEV_SWEEP_ALTERNATE ? h->sweep : 0;
+  h->sweep ^= 1;
   if (h->math_mode == LEV_MATH_ACCURATE)
     step_kernel<1><<<h->total_tiles, kTile, 0, h->stream>>>(a);
   else
@@ -340,6 +370,9 @@ int create_impl(LevEngine **out, int num_nets, const int32_t *Ns,
 
   // ---- validate shapes and lay out the packed arrays ----------------------
   long long node_off = 0, edge_off = 0, ring_off = 0, rp_off = 0;
+  long long slices = 0, sl_total = 0;
+  std::vector<long long> h_sl_off;
+  std::vector<int> h_sl_len;
   int tiles = 0;
   for (int n = 0; n < num_nets; ++n) {
     const int N = Ns[n], md = mds[n];
@@ -391,6 +424,23 @@ int create_impl(LevEngine **out, int num_nets, const int32_t *Ns,
       return rc;
     }
     params_to_desc(p, &d);
+    // ring gathers index a network's ring with 32-bit slot * Np + col
+    if ((unsigned long long)d.bsi * (unsigned long long)d.Np >= (1ull << 32)) {
+      delete h;
+      return fail(LEV_ERR_ARG, "network " + std::to_string(n) +
+                                   ": (max_delay + 2) * N must be below 2^32");
+    }
+    // SELL-32 slices: entry k of row i at sl_off[i/32] + 32k + i%32
+    d.slice_base = slices;
+    for (int s0 = 0; s0 < N; s0 += 32) {
+      int len = 0;
+      for (int i = s0; i < std::min(N, s0 + 32); ++i)
+        len = std::max(len, rp[i + 1] - rp[i]);
+      h_sl_off.push_back(sl_total);
+      h_sl_len.push_back(len);
+      sl_total += 32LL * len;
+      ++slices;
+    }
     h->net_E[n] = E;
     node_off += N;
     edge_off += E;
@@ -404,7 +454,8 @@ int create_impl(LevEngine **out, int num_nets, const int32_t *Ns,
   }
   h->total_nodes = node_off;
   h->total_edges = edge_off;
-  h->edge_alloc = (edge_off + 3) / 4 * 4 + 4;
+  h->num_slices = slices;
+  h->sl_total = sl_total;
   h->rp_total = rp_off;
   h->ring_floats = ring_off;
   h->total_tiles = tiles;
@@ -429,15 +480,17 @@ int create_impl(LevEngine **out, int num_nets, const int32_t *Ns,
     return fail(LEV_ERR_CUDA, std::string("cudaStreamCreate failed: ") +
                                   cudaGetErrorString(ce));
   }
-  int rc = LEV_OK;
+  int rc = prepare_step_kernels();
 #define LEV_ALLOC(ptr, count)                      \
   if (rc == LEV_OK) rc = dev_alloc(h, &(ptr), (count));
   LEV_ALLOC(h->d_nets, (size_t)num_nets);
   LEV_ALLOC(h->d_st, (size_t)num_nets);
   LEV_ALLOC(h->d_tiles, (size_t)tiles);
   LEV_ALLOC(h->d_row_ptr, (size_t)rp_off);
-  LEV_ALLOC(h->d_cd, (size_t)h->edge_alloc);
-  LEV_ALLOC(h->d_w, (size_t)h->edge_alloc);
+  LEV_ALLOC(h->d_sl_off, (size_t)slices);
+  LEV_ALLOC(h->d_sl_len, (size_t)slices);
+  LEV_ALLOC(h->d_sl_cd, (size_t)sl_total);
+  LEV_ALLOC(h->d_sl_w, (size_t)sl_total);
   LEV_ALLOC(h->d_theta, (size_t)node_off);
   LEV_ALLOC(h->d_theta_hat, (size_t)node_off);
   LEV_ALLOC(h->d_omega, (size_t)node_off);
@@ -464,10 +517,14 @@ int create_impl(LevEngine **out, int num_nets, const int32_t *Ns,
 
   // ---- uploads -------------------------------------------------------------
   unsigned *d_err = nullptr;
-  uint8_t *d_tmp = nullptr;
+  uint8_t *d_tmp = nullptr;    // delays, CSR order
+  int *d_tcol = nullptr;       // col_idx, CSR order
+  float *d_tw = nullptr;       // weights, CSR order
   auto cleanup_fail = [&](int code, const std::string &msg) {
     if (d_err) cudaFree(d_err);
     if (d_tmp) cudaFree(d_tmp);
+    if (d_tcol) cudaFree(d_tcol);
+    if (d_tw) cudaFree(d_tw);
     free_engine(h);
     return fail(code, msg);
   };
@@ -495,31 +552,36 @@ int create_impl(LevEngine **out, int num_nets, const int32_t *Ns,
     st[n].g = p.g;
   }
   LEV_UP(h->d_st, st.data(), sizeof(NetState) * num_nets);
-  if (cudaMemsetAsync(h->d_cd, 0, sizeof(uint32_t) * h->edge_alloc,
+  LEV_UP(h->d_sl_off, h_sl_off.data(), sizeof(long long) * slices);
+  LEV_UP(h->d_sl_len, h_sl_len.data(), sizeof(int) * slices);
+  // padding entries: node 0, delay 0, weight 0 (read, never used)
+  if (cudaMemsetAsync(h->d_sl_cd, 0, sizeof(uint32_t) * std::max<long long>(sl_total, 1),
                       h->stream) != cudaSuccess ||
-      cudaMemsetAsync(h->d_w, 0, sizeof(float) * h->edge_alloc, h->stream) !=
-          cudaSuccess ||
+      cudaMemsetAsync(h->d_sl_w, 0, sizeof(float) * std::max<long long>(sl_total, 1),
+                      h->stream) != cudaSuccess ||
       cudaMemsetAsync(h->d_ring, 0, sizeof(float) * std::max<long long>(ring_off, 1),
                       h->stream) != cudaSuccess)
     return cleanup_fail(LEV_ERR_CUDA, "memset failed");
 
   if (edge_off > 0) {
-    LEV_UP(h->d_w, w_cat, sizeof(float) * edge_off);
-    LEV_UP(h->d_cd, col_cat, sizeof(int32_t) * edge_off);
     if (cudaMalloc(&d_tmp, edge_off) != cudaSuccess ||
+        cudaMalloc(&d_tcol, sizeof(int) * edge_off) != cudaSuccess ||
+        cudaMalloc(&d_tw, sizeof(float) * edge_off) != cudaSuccess ||
         cudaMalloc(&d_err, sizeof(unsigned)) != cudaSuccess)
       return cleanup_fail(LEV_ERR_NOMEM, "temporary upload buffer");
+    LEV_UP(d_tw, w_cat, sizeof(float) * edge_off);
+    LEV_UP(d_tcol, col_cat, sizeof(int32_t) * edge_off);
     LEV_UP(d_tmp, d_cat, edge_off);
     if (cudaMemsetAsync(d_err, 0, sizeof(unsigned), h->stream) != cudaSuccess)
       return cleanup_fail(LEV_ERR_CUDA, "memset failed");
     for (int n = 0; n < num_nets; ++n) {
       const NetDesc &d = h->h_nets[n];
-      const long long E = h->net_E[n];
-      if (E == 0) continue;
-      int blocks = (int)std::min<long long>((E + 255) / 256, 148LL * 32);
-      pack_edges_kernel<<<blocks, 256, 0, h->stream>>>(
-          h->d_cd + d.edge_off, d_tmp + d.edge_off, E, d.N, d.max_delay,
-          d_err);
+      if (h->net_E[n] == 0) continue;
+      int blocks = (int)std::min<long long>((d.N + 255) / 256, 148LL * 16);
+      sell_convert_kernel<<<blocks, 256, 0, h->stream>>>(
+          0, h->d_row_ptr + d.rp_off, d.N, d.slice_base, h->d_sl_off,
+          d_tcol + d.edge_off, d_tmp + d.edge_off, d_tw + d.edge_off,
+          h->d_sl_cd, h->d_sl_w, d.max_delay, d_err);
     }
     unsigned herr = 0;
     cudaError_t e1 = cudaGetLastError();
@@ -537,8 +599,12 @@ int create_impl(LevEngine **out, int num_nets, const int32_t *Ns,
     if (herr & 2u)
       return cleanup_fail(LEV_ERR_ARG, "delay larger than max_delay");
     cudaFree(d_tmp);
+    cudaFree(d_tcol);
+    cudaFree(d_tw);
     cudaFree(d_err);
     d_tmp = nullptr;
+    d_tcol = nullptr;
+    d_tw = nullptr;
     d_err = nullptr;
   }
 #undef LEV_UP
@@ -766,12 +832,34 @@ int lev_set_theta_net(LevEngine *h, int32_t net, const float *theta_in) {
   return LEV_OK;
 }
 
+// Weights between the caller's CSR order and the engine's SELL-32 layout,
+// through a temporary device buffer in CSR order (mode 1: CSR -> SELL,
+// mode 2: SELL -> CSR).
+static int convert_weights(LevEngine *h, float *d_csr, int mode) {
+  for (int n = 0; n < h->num_nets; ++n) {
+    const NetDesc &d = h->h_nets[n];
+    if (h->net_E[n] == 0) continue;
+    int blocks = (int)std::min<long long>((d.N + 255) / 256, 148LL * 16);
+    sell_convert_kernel<<<blocks, 256, 0, h->stream>>>(
+        mode, h->d_row_ptr + d.rp_off, d.N, d.slice_base, h->d_sl_off,
+        nullptr, nullptr, d_csr + d.edge_off, h->d_sl_cd, h->d_sl_w,
+        d.max_delay, nullptr);
+  }
+  LEV_TRY_CUDA(cudaGetLastError());
+  return LEV_OK;
+}
+
 int lev_get_weights(LevEngine *h, float *w_out) {
   if (!h || (!w_out && h->total_edges > 0))
     return fail(LEV_ERR_ARG, "null argument");
   DeviceScope ds(h->device);
   if (h->total_edges == 0) return LEV_OK;
-  return copy_nodes(h, w_out, h->d_w, 0, h->total_edges);
+  float *tmp = nullptr;
+  LEV_TRY_CUDA(cudaMalloc(&tmp, sizeof(float) * h->total_edges));
+  int rc = convert_weights(h, tmp, 2);
+  if (rc == LEV_OK) rc = copy_nodes(h, w_out, tmp, 0, h->total_edges);
+  cudaFree(tmp);
+  return rc;
 }
 
 int lev_reset_weights(LevEngine *h, const float *w_in) {
@@ -779,9 +867,33 @@ int lev_reset_weights(LevEngine *h, const float *w_in) {
     return fail(LEV_ERR_ARG, "null argument");
   DeviceScope ds(h->device);
   if (h->total_edges == 0) return LEV_OK;
-  int rc = upload_nodes(h, h->d_w, w_in, 0, h->total_edges);
+  float *tmp = nullptr;
+  LEV_TRY_CUDA(cudaMalloc(&tmp, sizeof(float) * h->total_edges));
+  int rc = upload_nodes(h, tmp, w_in, 0, h->total_edges);
+  if (rc == LEV_OK) rc = convert_weights(h, tmp, 1);
+  cudaError_t ce = cudaStreamSynchronize(h->stream);
+  cudaFree(tmp);
   if (rc != LEV_OK) return rc;
-  LEV_TRY_CUDA(cudaStreamSynchronize(h->stream));
+  if (ce != cudaSuccess)
+    return fail(LEV_ERR_CUDA, std::string("reset_weights: ") + cudaGetErrorString(ce));
+  return LEV_OK;
+}
+
+int lev_selftest_wraps(uint64_t *mismatch_pm, uint64_t *mismatch_02) {
+  unsigned long long *d = nullptr;
+  LEV_TRY_CUDA(cudaMalloc(&d, 2 * sizeof(unsigned long long)));
+  unsigned long long hc[2] = {0, 0};
+  cudaError_t e = cudaMemset(d, 0, sizeof(hc));
+  if (e == cudaSuccess) {
+    selftest_wraps_kernel<<<148 * 8, 256>>>(d);
+    e = cudaGetLastError();
+  }
+  if (e == cudaSuccess) e = cudaMemcpy(hc, d, sizeof(hc), cudaMemcpyDeviceToHost);
+  cudaFree(d);
+  if (e != cudaSuccess)
+    return fail(LEV_ERR_CUDA, std::string("selftest: ") + cudaGetErrorString(e));
+  if (mismatch_pm) *mismatch_pm = hc[0];
+  if (mismatch_02) *mismatch_02 = hc[1];
   return LEV_OK;
 }
 

@@ -10,17 +10,27 @@
 //   host gain controller     :431-435  g update (moved on device)
 //
 // Work unit: a tile of 256 consecutive rows (nodes) of one network, one CTA
-// per tile; 256 = the reference block size (leviathan_kernel.cu:354) so the
-// block partial sums of cos/sin, and therefore r, are formed over the same
-// node groups and in the same tree order as the reference.
+// of 256 threads per tile, one thread per row -- the reference's mapping
+// (leviathan_kernel.cu:124, 354).  The block partial sums of cos/sin, and so
+// r, are formed over the same node groups in the same tree order.
 //
 // Layout in HBM (per network, packed over networks by offsets):
-//   row_ptr  int32 [N+1]      local CSR offsets (as given by the caller)
-//   cd       uint32[E]        (col_idx << 8) | delay  -- one 4-byte word
-//   w        f32   [E]        plastic weights, updated in place
+//   row_ptr  int32 [N+1]        local CSR offsets (as given by the caller)
+//   sl_cd    uint32[...]        (col_idx << 8) | delay, SELL-32 layout
+//   sl_w     f32   [...]        plastic weights, SELL-32 layout, in place
 //   theta, theta_hat, omega, omega_hat  f32 [N]
-//   ring     f32   [bsi][Np]  slot-major delay ring, bsi = max_delay + 2,
-//                             Np = N rounded up to 32 (128-byte rows)
+//   ring     f32   [bsi][Np]    slot-major delay ring, bsi = max_delay + 2,
+//                               Np = N rounded up to 32 (128-byte rows)
+//
+// SELL-32 (sliced ELLPACK, slice height 32): rows are grouped in slices of
+// 32 consecutive rows; a slice stores its rows' edges column-major, entry k
+// of the slice's row l at sl_off[slice] + 32*k + l, for k below the slice's
+// largest degree sl_len[slice] (shorter rows are padded with an inert entry).
+// Each warp owns one slice and each lane one row, so every load of the edge
+// streams is a coalesced 128-byte warp access, no lane ever searches for its
+// row, and a lane walks its row's edges in CSR order -- the order and the
+// fused multiply-add of the reference's per-row sum (:137-154), so the
+// coupling sum is bitwise the reference's.
 //
 // The ring has one slot more than the reference's max_delay+1: step t reads
 // slots (t-d) mod bsi for d in [0,max_delay] and writes theta(t+1) to slot
@@ -28,13 +38,6 @@
 // relies on separate launches for that ordering (:398 then :408); with the
 // extra slot one launch per step is race-free for every delay in
 // [0,max_delay] and the gathered values are identical.
-//
-// Edge phase: edges of the tile are processed flat (4 consecutive edges per
-// thread per iteration, 16-byte loads of cd and w, coalesced across the
-// warp); each edge finds its row in the staged row_ptr slice.  The coupling
-// term sum_e w_e*sin(d_e) of a row is then accumulated by the row's thread in
-// CSR order from shared memory, the same order and the same fused
-// multiply-add as the reference's per-row loop (:137-154).
 #pragma once
 
 #include <cuda_runtime.h>
@@ -44,13 +47,31 @@
 namespace lev {
 
 constexpr int kTile = 256;    // rows per CTA == threads per CTA
-constexpr int kChunk = 4096;  // edges staged in shared memory per pass
+constexpr int kChunk = 4096;  // edges staged in shared memory per pass (CSR kernels)
+
+// Build-time tuning of step_kernel (defaults are the measured best).
+#ifndef LEV_STEP_MINB
+#define LEV_STEP_MINB 3  // resident CTAs per SM the register budget targets
+#endif
+#ifndef LEV_SELL_UNROLL
+#define LEV_SELL_UNROLL 12  // edges per lane whose loads are in flight together
+#endif
+#ifndef LEV_SELL_PIPE
+#define LEV_SELL_PIPE 1  // 1: next group's edge streams load during this group
+#endif
+#ifndef LEV_RING_EVICT_LAST
+#define LEV_RING_EVICT_LAST 0  // 1: ring gathers carry an L2 evict_last policy
+#endif
+#ifndef LEV_RING_L2PF
+#define LEV_RING_L2PF 0  // 64/128/256: L2 fills that many bytes per ring miss
+#endif
 
 struct NetDesc {
   long long node_off;  // first node in the packed node arrays
-  long long edge_off;  // first edge in the packed edge arrays
+  long long edge_off;  // first edge in CSR order (packed over networks)
   long long ring_off;  // first float of the ring (multiple of 32)
   long long rp_off;    // first entry of the local row_ptr (N+1 entries)
+  long long slice_base;  // first SELL slice of this network
   int N;
   int Np;         // ring row pitch
   int bsi;        // ring slots = max_delay + 2
@@ -80,8 +101,10 @@ struct StepArgs {
   NetState *st;
   const int2 *tiles;  // (network, first local row)
   const int *row_ptr;
-  const uint32_t *cd;
-  float *w;
+  const long long *sl_off;  // per slice: first entry (multiple of 32)
+  const int *sl_len;        // per slice: largest degree
+  const uint32_t *sl_cd;
+  float *sl_w;
   float *theta;
   float *theta_hat;
   const float *omega;
@@ -93,6 +116,7 @@ struct StepArgs {
   int r_cap;
   int num_nets;
   float dt;
+  int reverse;  // 1: CTAs walk the tile list backwards (alternating sweeps)
 };
 
 // ---------------------------------------------------------------------------
@@ -100,16 +124,32 @@ struct StepArgs {
 // same form as leviathan_kernel.cu so that nvcc forms the same fused
 // multiply-adds; see the line cited at each use.
 // ---------------------------------------------------------------------------
+constexpr float kTwoPi = 2.0f * CUDART_PI_F;
+constexpr float kInvTwoPi = 0x1.45f306p-3f;  // RN(1 / kTwoPi)
+
+// x / kTwoPi, correctly rounded, without a division: q0 = RN(x * 1/c) is
+// corrected once with the exact remainder x - q0*c (one fma) -- the
+// division-by-a-known-divisor scheme of P. Markstein (IBM J. Res. Dev. 34,
+// 1990) and N. Brisebarre, J.-M. Muller, S. K. Raina (IEEE Trans. Comput.
+// 53(8), 2004).  For |x| >= 2^-100 the two phase wraps below computed with it
+// are bitwise identical to the same wraps computed with IEEE division, for
+// every float input; tiny |x| take the IEEE division.  lev_selftest_wraps()
+// re-checks that over all 2^32 inputs on the device.
+__device__ __forceinline__ float div_two_pi(float x) {
+  if (fabsf(x) < 0x1p-100f) return x / kTwoPi;
+  const float q0 = __fmul_rn(x, kInvTwoPi);
+  const float rem = __fmaf_rn(-q0, kTwoPi, x);
+  return __fmaf_rn(rem, kInvTwoPi, q0);
+}
+
 __device__ __forceinline__ float wrap_pm_pi(float diff) {
   // symmetric wrap to [-pi, pi): leviathan_kernel.cu:105 and :146
-  const float TWO_PI = 2.0f * CUDART_PI_F;
-  return diff - floorf(diff / TWO_PI + 0.5f) * TWO_PI;
+  return diff - floorf(div_two_pi(diff) + 0.5f) * kTwoPi;
 }
 
 __device__ __forceinline__ float wrap_0_2pi(float x) {
   // wrap to [0, 2pi): leviathan_kernel.cu:188
-  const float TWO_PI = 2.0f * CUDART_PI_F;
-  return x - floorf(x / TWO_PI) * TWO_PI;
+  return x - floorf(div_two_pi(x)) * kTwoPi;
 }
 
 template <int MATH>
@@ -136,43 +176,70 @@ __device__ __forceinline__ float gain_controller(float g, float r, float dt,
   return fmaxf(nd.g_min, fminf(nd.g_max, gn));
 }
 
+// Ring gather: read-only path; optionally with an L2 evict_last policy so
+// ring lines outlive the streamed edge arrays (which are loaded evict-first).
+__device__ __forceinline__ float ld_ring(const float *p, uint64_t pol) {
+#if LEV_RING_EVICT_LAST
+  float v;
+  asm("ld.global.nc.L2::cache_hint.f32 %0, [%1], %2;" : "=f"(v) : "l"(p), "l"(pol));
+  return v;
+#elif LEV_RING_L2PF == 64
+  (void)pol;
+  float v;
+  asm("ld.global.nc.L2::64B.f32 %0, [%1];" : "=f"(v) : "l"(p));
+  return v;
+#elif LEV_RING_L2PF == 128
+  (void)pol;
+  float v;
+  asm("ld.global.nc.L2::128B.f32 %0, [%1];" : "=f"(v) : "l"(p));
+  return v;
+#elif LEV_RING_L2PF == 256
+  (void)pol;
+  float v;
+  asm("ld.global.nc.L2::256B.f32 %0, [%1];" : "=f"(v) : "l"(p));
+  return v;
+#else
+  (void)pol;
+  return __ldg(p);
+#endif
+}
+
 // ---------------------------------------------------------------------------
 // The fused step.
 // ---------------------------------------------------------------------------
 template <int MATH>
-__global__ void __launch_bounds__(kTile, 3) step_kernel(const StepArgs a) {
-  __shared__ int s_rp[kTile + 1];
-  __shared__ float s_th[kTile];
-  __shared__ float s_ae[kTile];
-  __shared__ float2 s_ws[kChunk];
+__global__ void __launch_bounds__(kTile, LEV_STEP_MINB) step_kernel(const StepArgs a) {
   __shared__ float s_rc[32];
   __shared__ float s_rs[32];
   __shared__ int s_last;
 
   const int tid = threadIdx.x;
-  const int2 tile = a.tiles[blockIdx.x];
+  const int lane = tid & 31, warp = tid >> 5;
+  const int tix = a.reverse ? (int)(gridDim.x - 1 - blockIdx.x) : (int)blockIdx.x;
+  const int2 tile = a.tiles[tix];
   const NetDesc nd = a.nets[tile.x];
   NetState *ns = a.st + tile.x;
 
   const int N = nd.N;
   const int row0 = tile.y;
-  const int nrows = min(kTile, N - row0);
-  const long long node0 = nd.node_off + row0;
+  const int row = row0 + tid;
+  const bool live = row < N;
+  const long long gi = nd.node_off + row;
   const float dt = a.dt;
   const int bsi = nd.bsi;
   const int Np = nd.Np;
   const int cur = ns->cur;
   const float g = ns->g;
-  float *ring = a.ring + nd.ring_off;
-
-  // ---- stage this tile's row_ptr slice ------------------------------------
-  const int *rp = a.row_ptr + nd.rp_off + row0;
-  for (int k = tid; k <= nrows; k += kTile) s_rp[k] = __ldg(rp + k);
+  const float *ring = a.ring + nd.ring_off;
+  uint64_t ring_pol = 0;
+#if LEV_RING_EVICT_LAST
+  asm("createpolicy.fractional.L2::evict_last.b64 %0, 1.0;" : "=l"(ring_pol));
+#endif
 
   // ---- predictor (prep_kernel, leviathan_kernel.cu:100-110) ----------------
   float th = 0.0f, eps = 0.0f;
-  if (tid < nrows) {
-    const long long gi = node0 + tid;
+  int deg = 0;
+  if (live) {
     th = a.theta[gi];
     const float thh = a.theta_hat[gi];
     const float wh = a.omega_hat[gi];
@@ -181,102 +248,126 @@ __global__ void __launch_bounds__(kTile, 3) step_kernel(const StepArgs a) {
     eps = sinf(diff);
     a.theta_hat[gi] = thh + dt * wh;
     a.omega_hat[gi] = wh + nd.kappa_w * dt * eps;
+    const int *rp = a.row_ptr + nd.rp_off + row;
+    deg = rp[1] - rp[0];
   }
-  s_th[tid] = th;
-  s_ae[tid] = fabsf(eps);
-  __syncthreads();
+  const float my_eps = fabsf(eps);
 
-  // ---- edges (csr_physics_kernel, leviathan_kernel.cu:126-165) -------------
+  // ---- edges of this lane's row (csr_physics_kernel, :126-165) -------------
   const float eta = nd.eta, gamma = nd.gamma, lam = nd.lam;
   const float w_min = nd.w_min, w_max = nd.w_max;
-  const long long eoff = nd.edge_off;
-  const long long gbeg = eoff + s_rp[0];
-  const long long gend = eoff + s_rp[nrows];
-  const int my_rs = (tid < nrows) ? s_rp[tid] : 0;
-  const int my_re = (tid < nrows) ? s_rp[tid + 1] : 0;
-
   float local_sum = 0.0f;
-  int rlo = 0;  // row search lower bound, monotone in the edge index
-  const long long vstart = (gbeg < gend) ? (gbeg & ~3LL) : gend;
-  for (long long vc = vstart; vc < gend; vc += kChunk) {
-    const long long cend = min(vc + (long long)kChunk, gend);
-    for (long long g4 = vc + 4LL * tid; g4 < cend; g4 += 4LL * kTile) {
-      const uint4 p = __ldcs(reinterpret_cast<const uint4 *>(a.cd + g4));
-      const float4 wv = __ldcs(reinterpret_cast<const float4 *>(a.w + g4));
-      const uint32_t pq[4] = {p.x, p.y, p.z, p.w};
-      const float wq[4] = {wv.x, wv.y, wv.z, wv.w};
-      float wn[4] = {wv.x, wv.y, wv.z, wv.w};
-      // row of the first valid edge of this vector
-      const long long efirst = g4 > gbeg ? g4 : gbeg;
-      const int lef = (int)(efirst - eoff);
-      int lo = rlo, hi = nrows;
-      while (hi - lo > 1) {
-        const int mid = (lo + hi) >> 1;
-        if (s_rp[mid] <= lef) lo = mid; else hi = mid;
-      }
-      int r = lo;
-      bool full = true;
+  const int slice_row0 = row0 + 32 * warp;
+  if (slice_row0 < N) {  // warp-uniform
+    const long long s = nd.slice_base + (slice_row0 >> 5);
+    const int len = a.sl_len[s];
+    const long long base = a.sl_off[s] + lane;
+    const uint32_t *cdp = a.sl_cd + base;
+    float *wp = a.sl_w + base;
+    constexpr int U = LEV_SELL_UNROLL;
+#if LEV_SELL_PIPE
+    // software-pipelined: the edge streams of group k0+U are in flight
+    // while the ring gathers and math of group k0 run
+    uint32_t p[U];
+    float wv[U], dj[U];
 #pragma unroll
-      for (int q = 0; q < 4; ++q) {
-        const long long ge = g4 + q;
-        if (ge < gbeg || ge >= cend) { full = false; continue; }
-        const int le = (int)(ge - eoff);
-        while (s_rp[r + 1] <= le) ++r;
-        const int j = (int)(pq[q] >> 8);
-        const int d = (int)(pq[q] & 255u);
-        int slot = cur - d;
+    for (int u = 0; u < U; ++u) {
+      p[u] = (u < len) ? __ldcs(cdp + 32 * u) : 0u;
+      wv[u] = (u < len) ? __ldcs(wp + 32 * u) : 0.0f;
+    }
+    for (int k0 = 0; k0 < len; k0 += U) {
+#pragma unroll
+      for (int u = 0; u < U; ++u) {
+        int slot = cur - (int)(p[u] & 255u);
         slot += (slot < 0) ? bsi : 0;
-        const float delayed_j = __ldg(ring + (long long)slot * Np + j);
-        float diff = delayed_j - s_th[r];
-        diff = wrap_pm_pi(diff);
-        float w = wq[q];
-        float sin_diff, cos_diff;
-        lev_sincos<MATH>(diff, &sin_diff, &cos_diff);
-        s_ws[ge - vc] = make_float2(w, sin_diff);
-        const float my_eps = s_ae[r];
-        float dw = dt * (eta * cos_diff * (1.0f - gamma * my_eps) - lam * w);
-        w += dw;
-        if (!isfinite(w)) w = w_min;
-        w = fmaxf(w_min, fminf(w_max, w));
-        wn[q] = w;
+        dj[u] = ld_ring(ring + ((unsigned)slot * (unsigned)Np + (p[u] >> 8)), ring_pol);
       }
-      rlo = r;
-      if (full) {
-        __stcs(reinterpret_cast<float4 *>(a.w + g4),
-               make_float4(wn[0], wn[1], wn[2], wn[3]));
-      } else {
+      uint32_t pn[U];
+      float wn[U];
 #pragma unroll
-        for (int q = 0; q < 4; ++q) {
-          const long long ge = g4 + q;
-          if (ge >= gbeg && ge < cend) a.w[ge] = wn[q];
+      for (int u = 0; u < U; ++u) {
+        const int k = k0 + U + u;
+        pn[u] = (k < len) ? __ldcs(cdp + 32 * k) : 0u;
+        wn[u] = (k < len) ? __ldcs(wp + 32 * k) : 0.0f;
+      }
+#pragma unroll
+      for (int u = 0; u < U; ++u) {
+        if (k0 + u < deg) {
+          const float delayed_j = dj[u];
+          float diff = delayed_j - th;
+          diff = wrap_pm_pi(diff);
+          float w = wv[u];
+          float sin_diff, cos_diff;
+          lev_sincos<MATH>(diff, &sin_diff, &cos_diff);
+          local_sum += w * sin_diff;
+          float dw = dt * (eta * cos_diff * (1.0f - gamma * my_eps) - lam * w);
+          w += dw;
+          if (!isfinite(w)) w = w_min;
+          w = fmaxf(w_min, fminf(w_max, w));
+          __stcs(wp + 32 * (k0 + u), w);
+        }
+      }
+#pragma unroll
+      for (int u = 0; u < U; ++u) {
+        p[u] = pn[u];
+        wv[u] = wn[u];
+      }
+    }
+#else
+    for (int k0 = 0; k0 < len; k0 += U) {
+      // all U entries' stream loads, then all U ring gathers, are issued
+      // before the dependent math so their latencies overlap
+      uint32_t p[U];
+      float wv[U], dj[U];
+#pragma unroll
+      for (int u = 0; u < U; ++u) {
+        if (k0 + u < len) {  // warp-uniform
+          p[u] = __ldcs(cdp + 32 * (k0 + u));
+          wv[u] = __ldcs(wp + 32 * (k0 + u));
+        } else {
+          p[u] = 0u;
+          wv[u] = 0.0f;
+        }
+      }
+#pragma unroll
+      for (int u = 0; u < U; ++u) {
+        int slot = cur - (int)(p[u] & 255u);
+        slot += (slot < 0) ? bsi : 0;
+        // slot * Np + col < 2^32 is checked when the engine is created
+        dj[u] = ld_ring(ring + ((unsigned)slot * (unsigned)Np + (p[u] >> 8)), ring_pol);
+      }
+#pragma unroll
+      for (int u = 0; u < U; ++u) {
+        if (k0 + u < deg) {
+          const float delayed_j = dj[u];
+          float diff = delayed_j - th;
+          diff = wrap_pm_pi(diff);
+          float w = wv[u];
+          float sin_diff, cos_diff;
+          lev_sincos<MATH>(diff, &sin_diff, &cos_diff);
+          local_sum += w * sin_diff;
+          float dw = dt * (eta * cos_diff * (1.0f - gamma * my_eps) - lam * w);
+          w += dw;
+          if (!isfinite(w)) w = w_min;
+          w = fmaxf(w_min, fminf(w_max, w));
+          __stcs(wp + 32 * (k0 + u), w);
         }
       }
     }
-    __syncthreads();
-    // coupling sum of this thread's row, CSR order (leviathan_kernel.cu:154)
-    if (tid < nrows) {
-      const long long b = max(eoff + my_rs, vc);
-      const long long e = min(eoff + my_re, cend);
-      for (long long x = b; x < e; ++x) {
-        const float2 v = s_ws[x - vc];
-        local_sum += v.x * v.y;
-      }
-    }
-    __syncthreads();
+#endif
   }
 
   // ---- integrate (integrate_and_reduce_kernel, leviathan_kernel.cu:182-196)
   int nxt = cur + 1;
   if (nxt == bsi) nxt = 0;
   float my_cos = 0.0f, my_sin = 0.0f;
-  if (tid < nrows) {
-    const long long gi = node0 + tid;
+  if (live) {
     float inc = dt * (a.omega[gi] + g * local_sum - nd.alpha * eps);
     float x = th + inc;
     x = wrap_0_2pi(x);
     if (!isfinite(x)) x = 0.0f;
     a.theta[gi] = x;
-    ring[(long long)nxt * Np + row0 + tid] = x;
+    a.ring[nd.ring_off + (long long)nxt * Np + row] = x;
     lev_sincos<MATH>(x, &my_sin, &my_cos);
   }
 
@@ -287,7 +378,6 @@ __global__ void __launch_bounds__(kTile, 3) step_kernel(const StepArgs a) {
     my_cos += __shfl_down_sync(mask, my_cos, off);
     my_sin += __shfl_down_sync(mask, my_sin, off);
   }
-  const int lane = tid & 31, warp = tid >> 5;
   if (lane == 0) {
     s_rc[warp] = my_cos;
     s_rs[warp] = my_sin;
@@ -350,7 +440,7 @@ __global__ void __launch_bounds__(kTile, 3) step_kernel(const StepArgs a) {
 }
 
 // ---------------------------------------------------------------------------
-// Helpers
+// Layout conversion and helpers
 // ---------------------------------------------------------------------------
 
 // Every ring slot of every node := theta (init_buffer_kernel,
@@ -367,21 +457,41 @@ __global__ void ring_fill_kernel(const float *__restrict__ theta,
   }
 }
 
-// cd[e] := (col[e] << 8) | delay[e], in place over cd (which holds col on
-// entry).  Out-of-range columns or delays set bits of *err.
-__global__ void pack_edges_kernel(uint32_t *__restrict__ cd,
-                                  const uint8_t *__restrict__ delays,
-                                  long long E, int N, int max_delay,
-                                  unsigned *__restrict__ err) {
-  for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < E;
-       e += (long long)gridDim.x * blockDim.x) {
-    const int col = (int)cd[e];
-    const int d = delays[e];
+// CSR -> SELL-32 for one network: entry k of row i goes to
+// sl_off[slice_base + i/32] + 32k + i%32.  One thread per row.
+// mode 0: pack (col, delay) into sl_cd and copy weights, validating
+//         col in [0,N) and delay <= max_delay (bits of *err);
+// mode 1: weights only, CSR -> SELL;   mode 2: weights only, SELL -> CSR.
+__global__ void sell_convert_kernel(int mode, const int *__restrict__ row_ptr,
+                                    int N, long long slice_base,
+                                    const long long *__restrict__ sl_off,
+                                    const int *__restrict__ col,
+                                    const uint8_t *__restrict__ delays,
+                                    float *__restrict__ w_csr,
+                                    uint32_t *__restrict__ sl_cd,
+                                    float *__restrict__ sl_w, int max_delay,
+                                    unsigned *__restrict__ err) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < N;
+       i += gridDim.x * blockDim.x) {
+    const int e0 = row_ptr[i], e1 = row_ptr[i + 1];
+    const long long base = sl_off[slice_base + (i >> 5)] + (i & 31);
     unsigned bad = 0u;
-    if (col < 0 || col >= N) bad |= 1u;
-    if (d > max_delay) bad |= 2u;
+    for (int e = e0; e < e1; ++e) {
+      const long long idx = base + 32LL * (e - e0);
+      if (mode == 0) {
+        const int c = col[e];
+        const int d = delays[e];
+        if (c < 0 || c >= N) bad |= 1u;
+        if (d > max_delay) bad |= 2u;
+        sl_cd[idx] = ((uint32_t)c << 8) | (uint32_t)d;
+        sl_w[idx] = w_csr[e];
+      } else if (mode == 1) {
+        sl_w[idx] = w_csr[e];
+      } else {
+        w_csr[e] = sl_w[idx];
+      }
+    }
     if (bad) atomicOr(err, bad);
-    cd[e] = ((uint32_t)col << 8) | (uint32_t)d;
   }
 }
 
@@ -390,6 +500,30 @@ __global__ void reset_rpos_kernel(NetState *st, int num_nets) {
   for (int n = blockIdx.x * blockDim.x + threadIdx.x; n < num_nets;
        n += gridDim.x * blockDim.x)
     st[n].rpos = 0;
+}
+
+// Exhaustive check of the division-free phase wraps: for every float bit
+// pattern x, wrap_pm_pi(x) and wrap_0_2pi(x) against the same expressions
+// with IEEE division (leviathan_kernel.cu:105,146,188).  counts[0], counts[1]
+// receive the numbers of inputs whose results differ in any bit (NaN equal
+// to NaN).
+__global__ void selftest_wraps_kernel(unsigned long long *counts) {
+  const unsigned long long stride = (unsigned long long)gridDim.x * blockDim.x;
+  unsigned long long bad_pm = 0, bad_02 = 0;
+  for (unsigned long long k = blockIdx.x * (unsigned long long)blockDim.x + threadIdx.x;
+       k < (1ull << 32); k += stride) {
+    const float x = __uint_as_float((unsigned int)k);
+    const float ref_pm = x - floorf(x / kTwoPi + 0.5f) * kTwoPi;
+    const float ref_02 = x - floorf(x / kTwoPi) * kTwoPi;
+    const float got_pm = wrap_pm_pi(x);
+    const float got_02 = wrap_0_2pi(x);
+    const bool nan_pm = isnan(ref_pm) && isnan(got_pm);
+    const bool nan_02 = isnan(ref_02) && isnan(got_02);
+    bad_pm += (!nan_pm && __float_as_uint(ref_pm) != __float_as_uint(got_pm));
+    bad_02 += (!nan_02 && __float_as_uint(ref_02) != __float_as_uint(got_02));
+  }
+  if (bad_pm) atomicAdd(counts + 0, bad_pm);
+  if (bad_02) atomicAdd(counts + 1, bad_02);
 }
 
 }  // namespace lev

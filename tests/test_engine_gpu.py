@@ -93,6 +93,20 @@ def test_engine_bit_identical_to_reference_golden(case):
         np.testing.assert_array_equal(np.asarray(got), z[key], err_msg=key)
 
 
+def test_division_free_wraps_are_bitwise_ieee_for_all_inputs():
+    """The phase wraps evaluated without a division equal the reference's
+    IEEE-division expressions (leviathan_kernel.cu:105,146,188) in every bit,
+    for all 2^32 float inputs."""
+    import ctypes as C
+
+    from leviathan_v1_b200 import _lib
+
+    lib = _lib.load()
+    a, b = C.c_uint64(), C.c_uint64()
+    assert lib.lev_selftest_wraps(C.byref(a), C.byref(b)) == 0
+    assert a.value == 0 and b.value == 0, (a.value, b.value)
+
+
 # ---------------------------------------------------------------------------
 # Live reference engine (oracle/_ref) on larger inputs
 # ---------------------------------------------------------------------------
