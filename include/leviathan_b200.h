@@ -225,6 +225,57 @@ int lev_get_vram_usage(const LevEngine *h, size_t *bytes);
 int lev_selftest_wraps(uint64_t *mismatch_pm, uint64_t *mismatch_02);
 
 /* ------------------------------------------------------------------------ */
+/* Allocation-free step                                                      */
+/* ------------------------------------------------------------------------ */
+
+/* No counterpart in the reference (the reference engine always allocates its
+ * own state, leviathan_kernel.cu:315-368).
+ *
+ * For callers that cannot call cudaMalloc -- code whose device memory is
+ * owned by a memory planner or a framework allocator that must account for
+ * every byte, or a fixed-budget / real-time loop where cudaMalloc (which can
+ * synchronise the device and stall other streams) is not acceptable.  The
+ * caller owns every buffer; this call allocates nothing and frees nothing.
+ *
+ * One step of one network, enqueued on `stream` (a cudaStream_t; NULL = the
+ * legacy default stream); returns after the launch.  Same arithmetic and
+ * results as lev_step.  All array arguments are DEVICE pointers on the
+ * current device:
+ *   row_ptr[N+1], col_idx[E], delays[E]   CSR topology (must be valid: E =
+ *                                         row_ptr[N], col < N, delay <=
+ *                                         max_delay; out-of-range edges are
+ *                                         skipped, not read)
+ *   weights[E], theta[N], theta_hat[N], omega_hat[N]   state, updated
+ *   omega[N]                              natural frequencies
+ *   ring[(max_delay+2)*N]                 delay ring, slot-major: slot s of
+ *                                         node j at ring[s*N + j]; theta(t)
+ *                                         is in slot t mod (max_delay+2);
+ *                                         fill every slot with theta before
+ *                                         the first step (t = 0)
+ *   gain[1]   in: g for this step; out: g after the gain controller
+ *   r_out[1]  out: order parameter of the new phases
+ * t is the step index of the current phases (0 for the first call; the
+ * caller adds 1 after each call).  params is a host pointer (NULL:
+ * defaults).
+ *
+ * Scratch (one float2 per 256-node tile and a counter) lives in a fixed
+ * device array built into the library: N is limited to 4,194,304 nodes
+ * (LEV_ERR_ARG beyond), and every GPU that loads the library holds that
+ * array (about 128 KiB) until the process exits.  All calls share it and it
+ * keeps the last call's contents (the counter is cleared by each call), so
+ * calls whose kernels overlap on the GPU -- on different streams, or from
+ * different threads -- race and must not be issued.  The first call on a
+ * device looks up the array's device address (cudaGetSymbolAddress) with
+ * that device current; make that first call before any stream capture. */
+int lev_step_noalloc(int32_t N, int32_t max_delay, int64_t t,
+                     const int32_t *row_ptr, const int32_t *col_idx,
+                     const uint8_t *delays, float *weights, float *theta,
+                     float *theta_hat, const float *omega, float *omega_hat,
+                     float *ring, float *gain, float *r_out,
+                     const LevParams *params, float dt, int32_t math_mode,
+                     void *stream);
+
+/* ------------------------------------------------------------------------ */
 /* Reference C ABI (leviathan_kernel.cu:21-499), same symbols and signatures */
 /* ------------------------------------------------------------------------ */
 typedef struct LeviathanHandle LeviathanHandle;

@@ -100,6 +100,9 @@ PROTOTYPES = {
     "lev_set_math_mode": (C.c_int, [_P, _i32]),
     "lev_get_vram_usage": (C.c_int, [_P, C.POINTER(C.c_size_t)]),
     "lev_selftest_wraps": (C.c_int, [C.POINTER(C.c_uint64), C.POINTER(C.c_uint64)]),
+    "lev_step_noalloc":(C.c_int, [_i32, _i32, _i64, _P, _P, _P, _P, _P, _P, _P,
+                                   _P, _P, _P, _P, C.POINTER(LevParams), _f32,
+                                   _i32, _P]),
     # reference ABI (leviathan_kernel.cu:21-499)
     "leviathan_init": (_P, [C.c_int, C.c_int, _P, _P, _P, _P, _P, _P, _P]),
     "leviathan_step": (_f32, [_P, _f32]),

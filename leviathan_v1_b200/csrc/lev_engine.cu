@@ -1202,3 +1202,278 @@ LevEngine *leviathan_engine(LeviathanHandle *handle) {
 }
 
 }  // extern "C"
+
+// ===========================================================================
+// Allocation-free step: lev_step_noalloc
+//
+// For callers that cannot call cudaMalloc: code whose device memory is owned
+// by a memory planner or a framework allocator that must see every byte,
+// fixed-budget or real-time loops in which cudaMalloc (which may synchronise
+// the device and stall other streams) is not acceptable.  Such a caller keeps
+// the whole network state in its own device buffers; this entry point only
+// reads and writes them.  The step needs global scratch (one float2 partial
+// sum per 256-node tile and a completion ticket); it lives in the file-scope
+// device array below, of fixed size, which every GPU that loads this library
+// holds until the process exits.
+// ===========================================================================
+namespace lev {
+
+// Largest network the allocation-free step accepts (nodes).
+constexpr int kNoAllocMaxNodes = 1 << 22;  // 4,194,304
+constexpr int kNoAllocMaxTiles = kNoAllocMaxNodes / kTile;  // 16,384
+// [0, 2*kNoAllocMaxTiles): float2 partial sums; [2*kNoAllocMaxTiles]: ticket
+constexpr int kNoAllocWords = 2 * kNoAllocMaxTiles + 64;
+
+static __device__ __align__(256) unsigned int g_noalloc_scratch[kNoAllocWords];
+
+struct NoAllocArgs {
+  const int *row_ptr;
+  const int *col_idx;
+  const uint8_t *delays;
+  float *w;
+  float *theta;
+  float *theta_hat;
+  const float *omega;
+  float *omega_hat;
+  float *ring;  // [max_delay + 2][N]
+  float *gain;  // in: g for this step, out: g after the controller
+  float *r_out;
+  unsigned int *scratch;  // device address of g_noalloc_scratch
+  NetDesc nd;             // parameters (offsets unused)
+  int cur;                // ring slot of theta(t) = t mod (max_delay + 2)
+  float dt;
+};
+
+// Same arithmetic as step_kernel (one network, caller-owned buffers,
+// unpacked col_idx / delays, ring pitch N); scratch in g_noalloc_scratch.
+template <int MATH>
+__global__ void __launch_bounds__(kTile) noalloc_step_kernel(const NoAllocArgs a) {
+  __shared__ int s_rp[kTile + 1];
+  __shared__ float s_th[kTile];
+  __shared__ float s_ae[kTile];
+  __shared__ float2 s_ws[kChunk];
+  __shared__ float s_rc[32];
+  __shared__ float s_rs[32];
+  __shared__ int s_last;
+
+  const NetDesc &nd = a.nd;
+  const int tid = threadIdx.x;
+  const int N = nd.N;
+  const int row0 = blockIdx.x * kTile;
+  const int nrows = min(kTile, N - row0);
+  const float dt = a.dt;
+  const int bsi = nd.bsi;
+  const int cur = a.cur;
+  const float g = *a.gain;
+  float2 *partials = reinterpret_cast<float2 *>(a.scratch);
+  unsigned *ticket = a.scratch + 2 * kNoAllocMaxTiles;
+
+  for (int k = tid; k <= nrows; k += kTile) s_rp[k] = a.row_ptr[row0 + k];
+  float th = 0.0f, eps = 0.0f;
+  if (tid < nrows) {
+    const int gi = row0 + tid;
+    th = a.theta[gi];
+    const float thh = a.theta_hat[gi];
+    const float wh = a.omega_hat[gi];
+    float diff = th - thh;
+    diff = wrap_pm_pi(diff);
+    eps = sinf(diff);
+    a.theta_hat[gi] = thh + dt * wh;
+    a.omega_hat[gi] = wh + nd.kappa_w * dt * eps;
+  }
+  s_th[tid] = th;
+  s_ae[tid] = fabsf(eps);
+  __syncthreads();
+
+  const float eta = nd.eta, gamma = nd.gamma, lam = nd.lam;
+  const float w_min = nd.w_min, w_max = nd.w_max;
+  const int ebeg = s_rp[0], eend = s_rp[nrows];
+  const int my_rs = (tid < nrows) ? s_rp[tid] : 0;
+  const int my_re = (tid < nrows) ? s_rp[tid + 1] : 0;
+  float local_sum = 0.0f;
+  for (int c0 = ebeg; c0 < eend; c0 += kChunk) {
+    const int c1 = min(c0 + kChunk, eend);
+    int r = 0;
+    for (int e = c0 + tid; e < c1; e += kTile) {
+      int lo = r, hi = nrows;
+      while (hi - lo > 1) {
+        const int mid = (lo + hi) >> 1;
+        if (s_rp[mid] <= e) lo = mid; else hi = mid;
+      }
+      r = lo;
+      const int j = a.col_idx[e];
+      const int d = a.delays[e];
+      float w = a.w[e];
+      float sin_diff = 0.0f;
+      if ((unsigned)j < (unsigned)N && d <= nd.max_delay) {
+        int slot = cur - d;
+        slot += (slot < 0) ? bsi : 0;
+        const float delayed_j = a.ring[(long long)slot * N + j];
+        float diff = delayed_j - s_th[r];
+        diff = wrap_pm_pi(diff);
+        float cos_diff;
+        lev_sincos<MATH>(diff, &sin_diff, &cos_diff);
+        s_ws[e - c0] = make_float2(w, sin_diff);
+        const float my_eps = s_ae[r];
+        float dw = dt * (eta * cos_diff * (1.0f - gamma * my_eps) - lam * w);
+        w += dw;
+        if (!isfinite(w)) w = w_min;
+        w = fmaxf(w_min, fminf(w_max, w));
+        a.w[e] = w;
+      } else {
+        s_ws[e - c0] = make_float2(0.0f, 0.0f);  // out-of-range edge: skipped
+      }
+    }
+    __syncthreads();
+    if (tid < nrows) {
+      const int b = max(my_rs, c0), e = min(my_re, c1);
+      for (int x = b; x < e; ++x) {
+        const float2 v = s_ws[x - c0];
+        local_sum += v.x * v.y;
+      }
+    }
+    __syncthreads();
+  }
+
+  int nxt = cur + 1;
+  if (nxt == bsi) nxt = 0;
+  float my_cos = 0.0f, my_sin = 0.0f;
+  if (tid < nrows) {
+    const int gi = row0 + tid;
+    float inc = dt * (a.omega[gi] + g * local_sum - nd.alpha * eps);
+    float x = th + inc;
+    x = wrap_0_2pi(x);
+    if (!isfinite(x)) x = 0.0f;
+    a.theta[gi] = x;
+    a.ring[(long long)nxt * N + gi] = x;
+    lev_sincos<MATH>(x, &my_sin, &my_cos);
+  }
+  const unsigned mask = 0xffffffffu;
+#pragma unroll
+  for (int off = 16; off > 0; off /= 2) {
+    my_cos += __shfl_down_sync(mask, my_cos, off);
+    my_sin += __shfl_down_sync(mask, my_sin, off);
+  }
+  const int lane = tid & 31, warp = tid >> 5;
+  if (lane == 0) {
+    s_rc[warp] = my_cos;
+    s_rs[warp] = my_sin;
+  }
+  __syncthreads();
+  if (warp == 0) {
+    my_cos = (lane < (kTile / 32)) ? s_rc[lane] : 0.0f;
+    my_sin = (lane < (kTile / 32)) ? s_rs[lane] : 0.0f;
+#pragma unroll
+    for (int off = 16; off > 0; off /= 2) {
+      my_cos += __shfl_down_sync(mask, my_cos, off);
+      my_sin += __shfl_down_sync(mask, my_sin, off);
+    }
+    if (lane == 0) {
+      partials[blockIdx.x] = make_float2(my_cos, my_sin);
+      __threadfence();
+      const unsigned prev = atomicAdd(ticket, 1u);
+      s_last = (prev == gridDim.x - 1);
+    }
+  }
+  __syncthreads();
+  if (!s_last) return;
+  __threadfence();
+  if (warp == 0) {
+    float sum_cos = 0.0f, sum_sin = 0.0f;
+    for (int k = lane; k < (int)gridDim.x; k += 32) {
+      const float2 v = __ldcg(partials + k);
+      sum_cos += v.x;
+      sum_sin += v.y;
+    }
+#pragma unroll
+    for (int off = 16; off > 0; off /= 2) {
+      sum_cos += __shfl_down_sync(mask, sum_cos, off);
+      sum_sin += __shfl_down_sync(mask, sum_sin, off);
+    }
+    if (lane == 0) {
+      float inv_N = 1.0f / (float)N;
+      float r = sqrtf(sum_cos * sum_cos + sum_sin * sum_sin) * inv_N;
+      *a.gain = nd.ctrl ? gain_controller(g, r, dt, nd) : g;
+      *a.r_out = r;
+      *ticket = 0u;
+    }
+  }
+}
+
+// Device address of g_noalloc_scratch per device, looked up on the first
+// call made with that device current.
+constexpr int kNoAllocMaxDevices = 64;
+static unsigned int *g_noalloc_addr[kNoAllocMaxDevices] = {};
+
+}  // namespace lev
+
+extern "C" int lev_step_noalloc(int32_t N, int32_t max_delay, int64_t t,
+                                const int32_t *row_ptr, const int32_t *col_idx,
+                                const uint8_t *delays, float *weights,
+                                float *theta, float *theta_hat,
+                                const float *omega, float *omega_hat,
+                                float *ring, float *gain, float *r_out,
+                                const LevParams *params, float dt,
+                                int32_t math_mode, void *stream) {
+  if (N < 1 || N > kNoAllocMaxNodes)
+    return fail(LEV_ERR_ARG,
+                "lev_step_noalloc: N must be in [1, " +
+                    std::to_string(kNoAllocMaxNodes) +
+                    "] (size of the built-in scratch), got " + std::to_string(N));
+  if (max_delay < 0 || max_delay > 255)
+    return fail(LEV_ERR_ARG, "lev_step_noalloc: max_delay must be in [0,255]");
+  if (t < 0) return fail(LEV_ERR_ARG, "lev_step_noalloc: t must be >= 0");
+  if (!row_ptr || !theta || !theta_hat || !omega || !omega_hat || !ring ||
+      !gain || !r_out)
+    return fail(LEV_ERR_ARG, "lev_step_noalloc: null device pointer");
+  if (!std::isfinite(dt)) return fail(LEV_ERR_ARG, "lev_step_noalloc: dt is not finite");
+  if (math_mode != LEV_MATH_REFERENCE && math_mode != LEV_MATH_ACCURATE)
+    return fail(LEV_ERR_ARG, "lev_step_noalloc: math_mode must be 0 or 1");
+  LevParams p;
+  if (params) p = *params; else lev_default_params(&p);
+  int rc = check_params(p);
+  if (rc != LEV_OK) return rc;
+
+  int dev = 0;
+  LEV_TRY_CUDA(cudaGetDevice(&dev));
+  if (dev < 0 || dev >= kNoAllocMaxDevices)
+    return fail(LEV_ERR_ARG, "lev_step_noalloc: device ordinal too large");
+  if (!g_noalloc_addr[dev]) {
+    void *addr = nullptr;
+    LEV_TRY_CUDA(cudaGetSymbolAddress(&addr, g_noalloc_scratch));
+    g_noalloc_addr[dev] = static_cast<unsigned int *>(addr);
+  }
+  unsigned int *scratch = g_noalloc_addr[dev];
+  cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
+
+  NoAllocArgs a;
+  std::memset(&a, 0, sizeof(a));
+  a.row_ptr = row_ptr;
+  a.col_idx = col_idx;
+  a.delays = delays;
+  a.w = weights;
+  a.theta = theta;
+  a.theta_hat = theta_hat;
+  a.omega = omega;
+  a.omega_hat = omega_hat;
+  a.ring = ring;
+  a.gain = gain;
+  a.r_out = r_out;
+  a.scratch = scratch;
+  a.nd.N = N;
+  a.nd.bsi = max_delay + 2;
+  a.nd.max_delay = max_delay;
+  params_to_desc(p, &a.nd);
+  a.cur = (int)(t % (int64_t)(max_delay + 2));
+  a.dt = dt;
+  // the ticket must start at zero even if an earlier call was interrupted
+  LEV_TRY_CUDA(cudaMemsetAsync(scratch + 2 * kNoAllocMaxTiles, 0,
+                               sizeof(unsigned int), s));
+  const int tiles = (N + kTile - 1) / kTile;
+  if (math_mode == LEV_MATH_ACCURATE)
+    noalloc_step_kernel<1><<<tiles, kTile, 0, s>>>(a);
+  else
+    noalloc_step_kernel<0><<<tiles, kTile, 0, s>>>(a);
+  LEV_TRY_CUDA(cudaGetLastError());
+  return LEV_OK;
+}
