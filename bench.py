@@ -242,6 +242,73 @@ def fp64_error_small():
 
 
 # ---------------------------------------------------------------------------
+# batched sweep (512 networks, one launch per step, sharded over ranks)
+# ---------------------------------------------------------------------------
+def run_batched(args, rank, world, plain_value):
+    import torch
+
+    from leviathan_v1_b200 import BatchEngine, LeviathanEngine
+    from leviathan_v1_b200.graphs import batch_specs, build_batch
+    from leviathan_v1_b200.sharding import gather_results, shard_by_edges, summarize_r
+
+    specs = batch_specs(512, seed=0)
+    shards = shard_by_edges([s["E"] for s in specs], world)
+    mine = shards[rank]
+    nets, params = build_batch([specs[i] for i in mine])
+    E_local = sum(n.E for n in nets)
+    N_local = sum(n.N for n in nets)
+    eng = BatchEngine([n.as_dict() for n in nets], params=params)
+    tune = eng.autotune(DT, trial_steps=5)
+    S = args.batched_steps
+    eng.step_n_async(DT, max(args.warmup, 3))
+    eng.synchronize()
+    stream = torch.cuda.ExternalStream(eng.stream_ptr)
+    barrier(world)
+    torch.cuda.synchronize()
+    ev0 = torch.cuda.Event(enable_timing=True)
+    ev1 = torch.cuda.Event(enable_timing=True)
+    ev0.record(stream)
+    eng.step_n_async(DT, S)
+    ev1.record(stream)
+    ev1.synchronize()
+    barrier(world)
+    ms = max_over_ranks(ev0.elapsed_time(ev1), world)
+    E_tot = sum_over_ranks(E_local, world)
+    N_tot = sum_over_ranks(N_local, world)
+    value = E_tot * S / (ms / 1e3)
+    # r(K) curve: sweep continues to 1000 steps in total, mean r of the last 100
+    done = 3 + S
+    r = eng.step_n(DT, max(1000 - done, 100))
+    curve = gather_results(mine, summarize_r(r, 100), len(specs))
+    eng.close()
+    # the same networks one engine at a time (the reference's serial pattern,
+    # experiments/phase_sweep.py), a sample of 16 networks on this rank
+    sample = nets[:: max(1, len(nets) // 16)][:16]
+    t0 = time.perf_counter()
+    E_s = 0
+    for n, p in zip(sample, params[:: max(1, len(nets) // 16)][:16]):
+        e = LeviathanEngine(*n.engine_args(), params=p)
+        e.step_n(DT, 50)
+        E_s += n.E * 50
+        e.close()
+    serial = E_s / (time.perf_counter() - t0)
+    bins = np.linspace(0, 4, 9)
+    Ks = np.array([s["K"] for s in specs])
+    r_of_K = [float(np.nanmean(curve[(Ks >= lo) & (Ks < hi + (hi == 4)), 0]))
+              for lo, hi in zip(bins[:-1], bins[1:])]
+    return {"networks": len(specs), "nodes": int(N_tot), "edges": int(E_tot),
+            "steps": S, "ms_per_step": ms / S, "edge_updates_per_s": value,
+            "vs_plain_kernel": value / plain_value if plain_value else None,
+            "serial_engines_edge_updates_per_s": serial,
+            "serial_engines_note": "16 sampled networks, one engine each, 50 steps "
+                                   "per call incl. engine construction",
+            "autotune": {"chosen": tune["chosen"], "ms": tune["ms"],
+                         "variants": tune["variants"]},
+            "r_of_K_bins_0_to_4": r_of_K,
+            "algorithmic_bytes_per_step": int(17 * E_tot + 36 * N_tot)}
+
+
+# ---------------------------------------------------------------------------
 # our engine
 # ---------------------------------------------------------------------------
 def run_ours(args, rank, world, local):
@@ -323,6 +390,8 @@ def run_ours(args, rank, world, local):
         "r_final": r_last,
         "theta_finite": bool(np.all(np.isfinite(theta))),
     }
+    if not args.no_batched:
+        line["batched"] = run_batched(args, rank, world, value)
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline(net, budget_s=args.cpu_budget)
     if rank == 0 and not args.no_fp64_check:
@@ -401,6 +470,8 @@ def main():
     ap.add_argument("--cpu-budget", type=float, default=20.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-fp64-check", action="store_true")
+    ap.add_argument("--no-batched", action="store_true")
+    ap.add_argument("--batched-steps", type=int, default=200)
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3

@@ -216,6 +216,32 @@ int lev_set_math_mode(LevEngine *h, int32_t math_mode);
  * bytes actually allocated. */
 int lev_get_vram_usage(const LevEngine *h, size_t *bytes);
 
+/* ------------------------------------------------------------------------ */
+/* Autotuner (no reference counterpart)                                      */
+/* ------------------------------------------------------------------------ */
+
+/* The step kernel is compiled in several variants (edges per lane in flight,
+ * software pipelining, occupancy target).  An engine groups its networks in
+ * three degree classes by mean SELL slice length (<= 14, <= 26, larger); each
+ * class has its own tile list and variant.  Threads per row is fixed at one:
+ * the reference's CSR-order row sum needs a single thread per row. */
+int lev_num_variants(void);
+int lev_variant_info(int32_t v, int32_t *unroll, int32_t *pipelined,
+                     int32_t *min_blocks);
+int lev_class_info(const LevEngine *h, int32_t c, int32_t *ntiles,
+                   float *mean_slice_len, int64_t *edges, int32_t *variant);
+int lev_set_variant(LevEngine *h, int32_t c, int32_t v);
+
+/* Times every variant on every non-empty class of this engine
+ * (trial_steps steps each, after two warm-up steps), keeps the fastest per
+ * class, remembers it for later engines of the process with a similar class,
+ * and restores the engine state afterwards (device-side snapshot, so the
+ * simulation is unaffected).  variant_out[3] (may be NULL) receives the
+ * choices, ms_out[3 * lev_num_variants()] (may be NULL) the ms per step of
+ * every trial (0 for empty classes). */
+int lev_autotune(LevEngine *h, float dt, int32_t trial_steps,
+                 int32_t *variant_out, float *ms_out);
+
 /* Self-test of the phase wraps (no reference counterpart; checks this
  * library's division-free evaluation of the wraps of
  * leviathan_kernel.cu:105,146,188).  Runs, on the current device, both

@@ -99,7 +99,14 @@ PROTOTYPES = {
     "lev_get_params": (C.c_int, [_P, _i32, C.POINTER(LevParams)]),
     "lev_set_math_mode": (C.c_int, [_P, _i32]),
     "lev_get_vram_usage": (C.c_int, [_P, C.POINTER(C.c_size_t)]),
-    "lev_selftest_wraps": (C.c_int, [C.POINTER(C.c_uint64), C.POINTER(C.c_uint64)]),
+    "lev_num_variants": (C.c_int, []),
+    "lev_variant_info": (C.c_int, [_i32, C.POINTER(_i32), C.POINTER(_i32),
+                                   C.POINTER(_i32)]),
+    "lev_class_info": (C.c_int, [_P, _i32, C.POINTER(_i32), C.POINTER(_f32),
+                                 C.POINTER(_i64), C.POINTER(_i32)]),
+    "lev_set_variant": (C.c_int, [_P, _i32, _i32]),
+    "lev_autotune": (C.c_int, [_P, _f32, _i32, _P, _P]),
+    "lev_selftest_wraps":(C.c_int, [C.POINTER(C.c_uint64), C.POINTER(C.c_uint64)]),
     "lev_step_noalloc":(C.c_int, [_i32, _i32, _i64, _P, _P, _P, _P, _P, _P, _P,
                                    _P, _P, _P, _P, C.POINTER(LevParams), _f32,
                                    _i32, _P]),

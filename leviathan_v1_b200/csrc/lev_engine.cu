@@ -13,6 +13,7 @@
 #include <cstring>
 #include <limits>
 #include <map>
+#include <mutex>
 #include <string>
 #include <tuple>
 #include <vector>
@@ -56,6 +57,49 @@ struct GraphEntry {
   cudaGraph_t graph = nullptr;
   cudaGraphExec_t exec = nullptr;
 };
+
+// Compiled step-kernel variants the autotuner chooses from (see
+// step_kernel's template parameters).  Index 0 is the default.
+using StepFn = void (*)(StepArgs);
+struct StepVariant {
+  int U, PIPE, MINB;
+  StepFn fn[2];  // [math mode]
+};
+#define LEV_VARIANT(U, P, M) \
+  { U, P, M, { step_kernel<0, U, P, M>, step_kernel<1, U, P, M> } }
+static const StepVariant kVariants[] = {
+    LEV_VARIANT(12, 1, 3), LEV_VARIANT(8, 1, 3), LEV_VARIANT(16, 0, 3),
+    LEV_VARIANT(8, 0, 4),  LEV_VARIANT(4, 1, 4), LEV_VARIANT(6, 1, 4),
+};
+#undef LEV_VARIANT
+constexpr int kNumVariants = sizeof(kVariants) / sizeof(kVariants[0]);
+
+// Networks of a batch are grouped by the mean SELL slice length (the
+// per-lane edge count): each class has its own tile list and variant.
+constexpr int kNumClasses = 3;
+inline int degree_class(double mean_slice_len) {
+  return mean_slice_len <= 14.0 ? 0 : (mean_slice_len <= 26.0 ? 1 : 2);
+}
+
+struct TileClass {
+  int ntiles = 0;
+  int tile_off = 0;  // first entry of this class in the tile list
+  int variant = 0;
+  double mean_len = 0.0;  // mean slice length of the class
+  long long edges = 0;
+};
+
+// Autotuner results shared by the engines of a process, keyed by the degree
+// class, its mean slice length (rounded) and the size of its tile list
+// (power-of-two bucket).
+static std::mutex g_tune_mu;
+static std::map<std::tuple<int, int, int>, int> g_tune_cache;
+
+inline std::tuple<int, int, int> tune_key(const TileClass &tc, int c) {
+  int bucket = 0;
+  while ((1 << bucket) < tc.ntiles) ++bucket;
+  return std::make_tuple(c, (int)std::lround(tc.mean_len), bucket);
+}
 
 }  // namespace lev
 
@@ -105,6 +149,8 @@ struct LevEngine {
   size_t h_rstage_len = 0;
 
   std::map<std::tuple<int, uint32_t, int>, GraphEntry> graphs;
+
+  TileClass classes[kNumClasses];
 };
 
 struct LeviathanHandle {
@@ -241,31 +287,48 @@ StepArgs make_args(LevEngine *h, float dt, float *r_hist, int r_cap,
 // The step kernel keeps almost nothing in shared memory; prefer the largest
 // L1 carve-out so ring gathers reuse lines across a tile's rows.
 int prepare_step_kernels() {
-  LEV_TRY_CUDA(cudaFuncSetAttribute(step_kernel<0>,
-                                    cudaFuncAttributePreferredSharedMemoryCarveout,
-                                    (int)cudaSharedmemCarveoutMaxL1));
-  LEV_TRY_CUDA(cudaFuncSetAttribute(step_kernel<1>,
-                                    cudaFuncAttributePreferredSharedMemoryCarveout,
-                                    (int)cudaSharedmemCarveoutMaxL1));
+  for (int v = 0; v < kNumVariants; ++v)
+    for (int m = 0; m < 2; ++m)
+      LEV_TRY_CUDA(cudaFuncSetAttribute(
+          reinterpret_cast<const void *>(kVariants[v].fn[m]),
+          cudaFuncAttributePreferredSharedMemoryCarveout,
+          (int)cudaSharedmemCarveoutMaxL1));
   return LEV_OK;
 }
 
-// Launches one step.  Successive steps alternate the direction in which
-// CTAs walk the tile list, so the ring lines touched at the end of one step
-// are the first touched by the next while they are still in L2; results do
-// not depend on the direction.
-#ifndef LEV_SWEEP_ALTERNATE
-#define LEV_SWEEP_ALTERNATE 1
-#endif
-int launch_step(LevEngine *h, StepArgs a) {
-  a.reverse = LEV_SWEEP_ALTERNATE ? h->sweep : 0;
-  h->sweep ^= 1;
-  if (h->math_mode == LEV_MATH_ACCURATE)
-    step_kernel<1><<<h->total_tiles, kTile, 0, h->stream>>>(a);
-  else
-    step_kernel<0><<<h->total_tiles, kTile, 0, h->stream>>>(a);
-  LEV_TRY_CUDA(cudaGetLastError());
+int launch_class(LevEngine *h, int c, StepArgs a) {
+  const TileClass &tc = h->classes[c];
+  if (tc.ntiles == 0) return LEV_OK;
+  a.tiles = h->d_tiles + tc.tile_off;
+  const int mode = (h->math_mode == LEV_MATH_ACCURATE) ? 1 : 0;
+  void *args[] = {&a};
+  LEV_TRY_CUDA(cudaLaunchKernel(
+      reinterpret_cast<const void *>(kVariants[tc.variant].fn[mode]),
+      dim3(tc.ntiles), dim3(kTile), args, 0, h->stream));
   return LEV_OK;
+}
+
+// Launches one step: one kernel per degree class, each over its own tiles
+// with its own variant.  Successive steps alternate the direction in which
+// CTAs walk the tiles, so the ring lines touched at the end of one step are
+// the first touched by the next while they are still in L2; results do not
+// depend on the direction or on the variant.
+int launch_step(LevEngine *h, StepArgs a) {
+  a.reverse = h->sweep;
+  h->sweep ^= 1;
+  for (int c = 0; c < kNumClasses; ++c) {
+    int rc = launch_class(h, c, a);
+    if (rc != LEV_OK) return rc;
+  }
+  return LEV_OK;
+}
+
+void clear_graphs(LevEngine *h) {
+  for (auto &kv : h->graphs) {
+    if (kv.second.exec) cudaGraphExecDestroy(kv.second.exec);
+    if (kv.second.graph) cudaGraphDestroy(kv.second.graph);
+  }
+  h->graphs.clear();
 }
 
 // Graph of `len` steps (r history rows 0..len-1) keyed by (len, dt, mode).
@@ -278,13 +341,7 @@ int get_graph(LevEngine *h, int len, float dt, cudaGraphExec_t *out) {
     *out = it->second.exec;
     return LEV_OK;
   }
-  if (h->graphs.size() >= 16) {
-    for (auto &kv : h->graphs) {
-      cudaGraphExecDestroy(kv.second.exec);
-      cudaGraphDestroy(kv.second.graph);
-    }
-    h->graphs.clear();
-  }
+  if (h->graphs.size() >= 16) clear_graphs(h);
   GraphEntry ge;
   LEV_TRY_CUDA(
       cudaStreamBeginCapture(h->stream, cudaStreamCaptureModeThreadLocal));
@@ -460,11 +517,41 @@ int create_impl(LevEngine **out, int num_nets, const int32_t *Ns,
   h->ring_floats = ring_off;
   h->total_tiles = tiles;
 
-  std::vector<int2> h_tiles(tiles);
+  // Tile list grouped by degree class (class = mean SELL slice length of the
+  // network); within a class, networks keep their order.
+  std::vector<int> net_class(num_nets);
   for (int n = 0; n < num_nets; ++n) {
     const NetDesc &d = h->h_nets[n];
-    for (int t = 0; t < d.ntiles; ++t)
-      h_tiles[d.tile_off + t] = make_int2(n, t * kTile);
+    const long long s0 = d.slice_base, ns = (d.N + 31) / 32;
+    double sum = 0.0;
+    for (long long s = s0; s < s0 + ns; ++s) sum += h_sl_len[s];
+    const double mean = ns ? sum / ns : 0.0;
+    net_class[n] = degree_class(mean);
+    TileClass &tc = h->classes[net_class[n]];
+    tc.mean_len = (tc.mean_len * tc.ntiles + mean * d.ntiles) /
+                  std::max(1, tc.ntiles + d.ntiles);
+    tc.ntiles += d.ntiles;
+    tc.edges += h->net_E[n];
+  }
+  for (int c = 1; c < kNumClasses; ++c)
+    h->classes[c].tile_off = h->classes[c - 1].tile_off + h->classes[c - 1].ntiles;
+  std::vector<int2> h_tiles(tiles);
+  {
+    int fill[kNumClasses];
+    for (int c = 0; c < kNumClasses; ++c) fill[c] = h->classes[c].tile_off;
+    for (int n = 0; n < num_nets; ++n) {
+      const NetDesc &d = h->h_nets[n];
+      for (int t = 0; t < d.ntiles; ++t)
+        h_tiles[fill[net_class[n]]++] = make_int2(n, t * kTile);
+    }
+  }
+  {
+    // remembered choices of earlier engines with a similar class
+    std::lock_guard<std::mutex> lk(g_tune_mu);
+    for (int c = 0; c < kNumClasses; ++c) {
+      auto it = g_tune_cache.find(tune_key(h->classes[c], c));
+      h->classes[c].variant = (it != g_tune_cache.end()) ? it->second : 0;
+    }
   }
 
   // ---- device resources ----------------------------------------------------
@@ -1107,6 +1194,149 @@ int lev_set_math_mode(LevEngine *h, int32_t math_mode) {
     return fail(LEV_ERR_ARG, "math_mode must be 0 (reference) or 1");
   h->math_mode = math_mode;
   return LEV_OK;
+}
+
+int lev_num_variants(void) { return kNumVariants; }
+
+int lev_variant_info(int32_t v, int32_t *unroll, int32_t *pipelined,
+                     int32_t *min_blocks) {
+  if (v < 0 || v >= kNumVariants) return fail(LEV_ERR_ARG, "variant out of range");
+  if (unroll) *unroll = kVariants[v].U;
+  if (pipelined) *pipelined = kVariants[v].PIPE;
+  if (min_blocks) *min_blocks = kVariants[v].MINB;
+  return LEV_OK;
+}
+
+int lev_class_info(const LevEngine *h, int32_t c, int32_t *ntiles,
+                   float *mean_slice_len, int64_t *edges, int32_t *variant) {
+  if (!h) return fail(LEV_ERR_ARG, "null handle");
+  if (c < 0 || c >= kNumClasses) return fail(LEV_ERR_ARG, "class out of range");
+  const TileClass &tc = h->classes[c];
+  if (ntiles) *ntiles = tc.ntiles;
+  if (mean_slice_len) *mean_slice_len = (float)tc.mean_len;
+  if (edges) *edges = tc.edges;
+  if (variant) *variant = tc.variant;
+  return LEV_OK;
+}
+
+int lev_set_variant(LevEngine *h, int32_t c, int32_t v) {
+  if (!h) return fail(LEV_ERR_ARG, "null handle");
+  if (c < 0 || c >= kNumClasses) return fail(LEV_ERR_ARG, "class out of range");
+  if (v < 0 || v >= kNumVariants) return fail(LEV_ERR_ARG, "variant out of range");
+  if (h->classes[c].variant != v) {
+    DeviceScope ds(h->device);
+    cudaStreamSynchronize(h->stream);
+    clear_graphs(h);
+    h->classes[c].variant = v;
+  }
+  return LEV_OK;
+}
+
+// Device-side copy of the evolving state (weights, node state, ring,
+// per-network state) so tuning trials leave the simulation untouched.
+struct StateSnapshot {
+  float *w = nullptr, *th = nullptr, *thh = nullptr, *wh = nullptr,
+        *ring = nullptr;
+  NetState *st = nullptr;
+  void release() {
+    cudaFree(w);
+    cudaFree(th);
+    cudaFree(thh);
+    cudaFree(wh);
+    cudaFree(ring);
+    cudaFree(st);
+    w = th = thh = wh = ring = nullptr;
+    st = nullptr;
+  }
+};
+
+static int snapshot_copy(LevEngine *h, StateSnapshot &s, bool save) {
+  auto cp = [&](void *dst_save, void *live, size_t bytes) -> cudaError_t {
+    return save ? cudaMemcpyAsync(dst_save, live, bytes, cudaMemcpyDeviceToDevice, h->stream)
+                : cudaMemcpyAsync(live, dst_save, bytes, cudaMemcpyDeviceToDevice, h->stream);
+  };
+  const size_t nn = sizeof(float) * h->total_nodes;
+  cudaError_t e = cp(s.w, h->d_sl_w, sizeof(float) * std::max<long long>(h->sl_total, 1));
+  if (e == cudaSuccess) e = cp(s.th, h->d_theta, nn);
+  if (e == cudaSuccess) e = cp(s.thh, h->d_theta_hat, nn);
+  if (e == cudaSuccess) e = cp(s.wh, h->d_omega_hat, nn);
+  if (e == cudaSuccess) e = cp(s.ring, h->d_ring, sizeof(float) * h->ring_floats);
+  if (e == cudaSuccess) e = cp(s.st, h->d_st, sizeof(NetState) * h->num_nets);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(h->stream);
+  if (e != cudaSuccess)
+    return fail(LEV_ERR_CUDA, std::string("state snapshot: ") + cudaGetErrorString(e));
+  return LEV_OK;
+}
+
+int lev_autotune(LevEngine *h, float dt, int32_t trial_steps,
+                 int32_t *variant_out, float *ms_out) {
+  if (!h) return fail(LEV_ERR_ARG, "null handle");
+  if (trial_steps < 1) return fail(LEV_ERR_ARG, "trial_steps must be >= 1");
+  if (!std::isfinite(dt)) return fail(LEV_ERR_ARG, "dt is not finite");
+  DeviceScope ds(h->device);
+  LEV_TRY_CUDA(cudaStreamSynchronize(h->stream));
+  StateSnapshot snap;
+  const size_t nn = sizeof(float) * std::max<long long>(h->total_nodes, 1);
+  if (cudaMalloc(&snap.w, sizeof(float) * std::max<long long>(h->sl_total, 1)) != cudaSuccess ||
+      cudaMalloc(&snap.th, nn) != cudaSuccess || cudaMalloc(&snap.thh, nn) != cudaSuccess ||
+      cudaMalloc(&snap.wh, nn) != cudaSuccess ||
+      cudaMalloc(&snap.ring, sizeof(float) * std::max<long long>(h->ring_floats, 1)) != cudaSuccess ||
+      cudaMalloc(&snap.st, sizeof(NetState) * h->num_nets) != cudaSuccess) {
+    snap.release();
+    return fail(LEV_ERR_NOMEM, "autotune: no room for a state snapshot");
+  }
+  int rc = snapshot_copy(h, snap, true);
+  cudaEvent_t e0 = nullptr, e1 = nullptr;
+  if (rc == LEV_OK && (cudaEventCreate(&e0) != cudaSuccess || cudaEventCreate(&e1) != cudaSuccess))
+    rc = fail(LEV_ERR_CUDA, "autotune: event creation failed");
+  StepArgs a = make_args(h, dt, nullptr, 0, nullptr);
+  for (int c = 0; c < kNumClasses && rc == LEV_OK; ++c) {
+    TileClass &tc = h->classes[c];
+    if (tc.ntiles == 0) {
+      for (int v = 0; v < kNumVariants; ++v)
+        if (ms_out) ms_out[c * kNumVariants + v] = 0.0f;
+      continue;
+    }
+    float best = 0.0f;
+    int best_v = tc.variant;
+    for (int v = 0; v < kNumVariants && rc == LEV_OK; ++v) {
+      tc.variant = v;
+      for (int i = 0; i < 2 && rc == LEV_OK; ++i) {  // warm-up
+        a.reverse = i & 1;
+        rc = launch_class(h, c, a);
+      }
+      if (rc != LEV_OK) break;
+      cudaEventRecord(e0, h->stream);
+      for (int i = 0; i < trial_steps && rc == LEV_OK; ++i) {
+        a.reverse = i & 1;
+        rc = launch_class(h, c, a);
+      }
+      cudaEventRecord(e1, h->stream);
+      if (cudaEventSynchronize(e1) != cudaSuccess) {
+        rc = fail(LEV_ERR_CUDA, "autotune: trial failed");
+        break;
+      }
+      float ms = 0.0f;
+      cudaEventElapsedTime(&ms, e0, e1);
+      ms /= trial_steps;
+      if (ms_out) ms_out[c * kNumVariants + v] = ms;
+      if (v == 0 || ms < best) {
+        best = ms;
+        best_v = v;
+      }
+    }
+    tc.variant = best_v;
+    if (variant_out) variant_out[c] = best_v;
+    std::lock_guard<std::mutex> lk(g_tune_mu);
+    g_tune_cache[tune_key(tc, c)] = best_v;
+  }
+  if (e0) cudaEventDestroy(e0);
+  if (e1) cudaEventDestroy(e1);
+  if (rc == LEV_OK) rc = snapshot_copy(h, snap, false);
+  else snapshot_copy(h, snap, false);
+  snap.release();
+  clear_graphs(h);
+  return rc;
 }
 
 int lev_get_vram_usage(const LevEngine *h, size_t *bytes) {

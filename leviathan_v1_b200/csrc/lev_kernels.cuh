@@ -49,22 +49,11 @@ namespace lev {
 constexpr int kTile = 256;    // rows per CTA == threads per CTA
 constexpr int kChunk = 4096;  // edges staged in shared memory per pass (CSR kernels)
 
-// Build-time tuning of step_kernel (defaults are the measured best).
-#ifndef LEV_STEP_MINB
-#define LEV_STEP_MINB 3  // resident CTAs per SM the register budget targets
-#endif
-#ifndef LEV_SELL_UNROLL
-#define LEV_SELL_UNROLL 12  // edges per lane whose loads are in flight together
-#endif
-#ifndef LEV_SELL_PIPE
-#define LEV_SELL_PIPE 1  // 1: next group's edge streams load during this group
-#endif
-#ifndef LEV_RING_EVICT_LAST
-#define LEV_RING_EVICT_LAST 0  // 1: ring gathers carry an L2 evict_last policy
-#endif
-#ifndef LEV_RING_L2PF
-#define LEV_RING_L2PF 0  // 64/128/256: L2 fills that many bytes per ring miss
-#endif
+// step_kernel is instantiated for several (U, PIPE, MINB) variants, chosen per
+// engine (and per degree class of a batch) by the autotuner in lev_engine.cu:
+//   U     edges per lane whose loads are in flight together ("vector width")
+//   PIPE  1: the next group's edge-stream loads overlap this group's gathers
+//   MINB  resident CTAs per SM the register budget is sized for
 
 struct NetDesc {
   long long node_off;  // first node in the packed node arrays
@@ -176,39 +165,15 @@ __device__ __forceinline__ float gain_controller(float g, float r, float dt,
   return fmaxf(nd.g_min, fminf(nd.g_max, gn));
 }
 
-// Ring gather: read-only path; optionally with an L2 evict_last policy so
-// ring lines outlive the streamed edge arrays (which are loaded evict-first).
-__device__ __forceinline__ float ld_ring(const float *p, uint64_t pol) {
-#if LEV_RING_EVICT_LAST
-  float v;
-  asm("ld.global.nc.L2::cache_hint.f32 %0, [%1], %2;" : "=f"(v) : "l"(p), "l"(pol));
-  return v;
-#elif LEV_RING_L2PF == 64
-  (void)pol;
-  float v;
-  asm("ld.global.nc.L2::64B.f32 %0, [%1];" : "=f"(v) : "l"(p));
-  return v;
-#elif LEV_RING_L2PF == 128
-  (void)pol;
-  float v;
-  asm("ld.global.nc.L2::128B.f32 %0, [%1];" : "=f"(v) : "l"(p));
-  return v;
-#elif LEV_RING_L2PF == 256
-  (void)pol;
-  float v;
-  asm("ld.global.nc.L2::256B.f32 %0, [%1];" : "=f"(v) : "l"(p));
-  return v;
-#else
-  (void)pol;
-  return __ldg(p);
-#endif
-}
+// Ring gather: read-only (non-coherent) path.  The slot written by the same
+// launch is never read by it (see the ring note at the top).
+__device__ __forceinline__ float ld_ring(const float *p) { return __ldg(p); }
 
 // ---------------------------------------------------------------------------
 // The fused step.
 // ---------------------------------------------------------------------------
-template <int MATH>
-__global__ void __launch_bounds__(kTile, LEV_STEP_MINB) step_kernel(const StepArgs a) {
+template <int MATH, int U, int PIPE, int MINB>
+__global__ void __launch_bounds__(kTile, MINB) step_kernel(const StepArgs a) {
   __shared__ float s_rc[32];
   __shared__ float s_rs[32];
   __shared__ int s_last;
@@ -231,10 +196,6 @@ __global__ void __launch_bounds__(kTile, LEV_STEP_MINB) step_kernel(const StepAr
   const int cur = ns->cur;
   const float g = ns->g;
   const float *ring = a.ring + nd.ring_off;
-  uint64_t ring_pol = 0;
-#if LEV_RING_EVICT_LAST
-  asm("createpolicy.fractional.L2::evict_last.b64 %0, 1.0;" : "=l"(ring_pol));
-#endif
 
   // ---- predictor (prep_kernel, leviathan_kernel.cu:100-110) ----------------
   float th = 0.0f, eps = 0.0f;
@@ -264,8 +225,7 @@ __global__ void __launch_bounds__(kTile, LEV_STEP_MINB) step_kernel(const StepAr
     const long long base = a.sl_off[s] + lane;
     const uint32_t *cdp = a.sl_cd + base;
     float *wp = a.sl_w + base;
-    constexpr int U = LEV_SELL_UNROLL;
-#if LEV_SELL_PIPE
+    if constexpr (PIPE) {
     // software-pipelined: the edge streams of group k0+U are in flight
     // while the ring gathers and math of group k0 run
     uint32_t p[U];
@@ -280,7 +240,7 @@ __global__ void __launch_bounds__(kTile, LEV_STEP_MINB) step_kernel(const StepAr
       for (int u = 0; u < U; ++u) {
         int slot = cur - (int)(p[u] & 255u);
         slot += (slot < 0) ? bsi : 0;
-        dj[u] = ld_ring(ring + ((unsigned)slot * (unsigned)Np + (p[u] >> 8)), ring_pol);
+        dj[u] = ld_ring(ring + ((unsigned)slot * (unsigned)Np + (p[u] >> 8)));
       }
       uint32_t pn[U];
       float wn[U];
@@ -313,7 +273,7 @@ __global__ void __launch_bounds__(kTile, LEV_STEP_MINB) step_kernel(const StepAr
         wv[u] = wn[u];
       }
     }
-#else
+    } else {
     for (int k0 = 0; k0 < len; k0 += U) {
       // all U entries' stream loads, then all U ring gathers, are issued
       // before the dependent math so their latencies overlap
@@ -334,7 +294,7 @@ __global__ void __launch_bounds__(kTile, LEV_STEP_MINB) step_kernel(const StepAr
         int slot = cur - (int)(p[u] & 255u);
         slot += (slot < 0) ? bsi : 0;
         // slot * Np + col < 2^32 is checked when the engine is created
-        dj[u] = ld_ring(ring + ((unsigned)slot * (unsigned)Np + (p[u] >> 8)), ring_pol);
+        dj[u] = ld_ring(ring + ((unsigned)slot * (unsigned)Np + (p[u] >> 8)));
       }
 #pragma unroll
       for (int u = 0; u < U; ++u) {
@@ -354,7 +314,7 @@ __global__ void __launch_bounds__(kTile, LEV_STEP_MINB) step_kernel(const StepAr
         }
       }
     }
-#endif
+    }
   }
 
   // ---- integrate (integrate_and_reduce_kernel, leviathan_kernel.cu:182-196)

@@ -34,6 +34,14 @@ def _as(a, dtype) -> np.ndarray:
     return np.ascontiguousarray(np.asarray(a), dtype=dtype)
 
 
+def variant_info(v: int) -> dict:
+    """Tuning parameters of compiled step-kernel variant ``v``."""
+    lib = _lib.load()
+    u, p, m = C.c_int32(), C.c_int32(), C.c_int32()
+    check(lib.lev_variant_info(int(v), C.byref(u), C.byref(p), C.byref(m)))
+    return dict(unroll=u.value, pipelined=p.value, min_blocks=m.value)
+
+
 class _EngineBase:
     """Shared handle management and state access of both engine kinds."""
 
@@ -234,6 +242,34 @@ class _EngineBase:
         b = C.c_size_t()
         check(self._lib.lev_get_vram_usage(self.handle, C.byref(b)))
         return b.value
+
+    # -- autotuner ----------------------------------------------------------
+    def tuning(self) -> list:
+        """Degree classes of this engine: tiles, mean slice length, edges and
+        the step-kernel variant (unroll, pipelined, min_blocks) in use."""
+        out = []
+        for c in range(3):
+            nt, ml, ed, v = C.c_int32(), C.c_float(), C.c_int64(), C.c_int32()
+            check(self._lib.lev_class_info(self.handle, c, C.byref(nt), C.byref(ml),
+                                           C.byref(ed), C.byref(v)))
+            out.append(dict(cls=c, tiles=nt.value, mean_slice_len=ml.value,
+                            edges=ed.value, variant=v.value, **variant_info(v.value)))
+        return out
+
+    def autotune(self, dt: float = 0.05, trial_steps: int = 5) -> dict:
+        """Time every compiled variant per degree class, keep the fastest;
+        the simulation state is restored afterwards."""
+        nv = self._lib.lev_num_variants()
+        chosen = (C.c_int32 * 3)()
+        ms = (C.c_float * (3 * nv))()
+        check(self._lib.lev_autotune(self.handle, C.c_float(dt), int(trial_steps),
+                                     chosen, ms))
+        return dict(chosen=list(chosen),
+                    ms=[[ms[c * nv + v] for v in range(nv)] for c in range(3)],
+                    variants=[variant_info(v) for v in range(nv)])
+
+    def set_variant(self, cls: int, variant: int) -> None:
+        check(self._lib.lev_set_variant(self.handle, int(cls), int(variant)))
 
     # -- checkpoint ---------------------------------------------------------
     def get_state(self) -> dict:

@@ -182,21 +182,35 @@ def config_scale(seed: int = 0, N: int = 1_000_000, k: int = 32) -> Network:
     return make_network(N, k, 0.1, 64, seed)
 
 
+def batch_specs(num: int = 512, seed: int = 0, n_lo: int = 500,
+                n_hi: int = 50_000, ks=(8, 16, 20, 32)):
+    """Specifications of the batched sweep without building the graphs:
+    list of dicts (N, k, seed, K, E).  E = N*k exactly (WS rewiring moves
+    edges, it never adds or removes them)."""
+    rng = np.random.default_rng([seed, 0xBA7C4])
+    specs = []
+    for b in range(num):
+        N = int(round(math.exp(rng.uniform(math.log(n_lo), math.log(n_hi)))))
+        k = int(rng.choice(ks))
+        k = min(k, N - 2 - (N % 2))
+        K = 4.0 * b / max(num - 1, 1)
+        specs.append(dict(index=b, N=N, k=k, seed=seed * 100003 + b, K=K, E=N * k))
+    return specs
+
+
+def build_batch(specs):
+    """Networks and parameters (K swept, controller off) of ``specs``."""
+    nets = [make_network(s["N"], s["k"], 0.1, 50, s["seed"]) for s in specs]
+    params = [dict(g=s["K"], gain_controller=0) for s in specs]
+    return nets, params
+
+
 def config_batch(num: int = 512, seed: int = 0, n_lo: int = 500,
                  n_hi: int = 50_000, ks=(8, 16, 20, 32)):
     """Batched sweep: ``num`` networks, N log-uniform in [n_lo, n_hi], k
     uniform in ``ks``, p=0.1, delays [1,50]; coupling K swept linearly over
     [0, 4] with the controller off.  Returns (networks, params)."""
-    rng = np.random.default_rng([seed, 0xBA7C4])
-    nets, params = [], []
-    for b in range(num):
-        N = int(round(math.exp(rng.uniform(math.log(n_lo), math.log(n_hi)))))
-        k = int(rng.choice(ks))
-        k = min(k, N - 2 - (N % 2))
-        nets.append(make_network(N, k, 0.1, 50, seed * 100003 + b))
-        K = 4.0 * b / max(num - 1, 1)
-        params.append(dict(g=K, gain_controller=0))
-    return nets, params
+    return build_batch(batch_specs(num, seed, n_lo, n_hi, ks))
 
 
 def config_adjoint(seed: int = 0, N: int = 10_000, k: int = 20) -> Network:

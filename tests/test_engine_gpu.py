@@ -198,6 +198,30 @@ def test_batch_equals_individual_engines():
     be.close()
 
 
+def test_autotune_leaves_simulation_unchanged():
+    nets = [make_network(n, k, 0.1, 20, seed=s)
+            for n, k, s in [(3000, 8, 1), (2000, 20, 2), (5000, 32, 3)]]
+    a = BatchEngine([n.as_dict() for n in nets])
+    b = BatchEngine([n.as_dict() for n in nets])
+    classes = [c for c in a.tuning() if c["tiles"]]
+    assert len(classes) == 3  # k = 8, 20, 32 fall in three degree classes
+    ra = [a.step_n(DT, 20)]
+    res = a.autotune(DT, trial_steps=3)
+    assert all(0 <= v < len(res["variants"]) for v in res["chosen"])
+    ra.append(a.step_n(DT, 30))
+    rb = b.step_n(DT, 50)
+    np.testing.assert_array_equal(np.concatenate(ra), rb)
+    np.testing.assert_array_equal(a.get_theta(), b.get_theta())
+    np.testing.assert_array_equal(a.get_weights(), b.get_weights())
+    for c in range(3):  # every variant gives the same bits
+        for v in range(len(res["variants"])):
+            b.set_variant(c, v)
+            a.set_variant(c, (v + 1) % len(res["variants"]))
+            np.testing.assert_array_equal(a.step_n(DT, 2), b.step_n(DT, 2))
+    a.close()
+    b.close()
+
+
 def test_checkpoint_round_trip_is_exact():
     net = make_network(5000, 16, 0.1, 40, seed=8)
     e = LeviathanEngine(*net.engine_args())
