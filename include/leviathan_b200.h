@@ -242,6 +242,40 @@ int lev_set_variant(LevEngine *h, int32_t c, int32_t v);
 int lev_autotune(LevEngine *h, float dt, int32_t trial_steps,
                  int32_t *variant_out, float *ms_out);
 
+/* ------------------------------------------------------------------------ */
+/* Adjoint: gradients through T steps (no reference counterpart)             */
+/* ------------------------------------------------------------------------ */
+
+/* Differentiable run of an engine's networks from the phases and predictor
+ * phases the engine holds when the adjoint is created, with
+ * omega_hat(0) = omega (leviathan_kernel.cu:350), every ring slot =
+ * theta(0), and the inputs: omega[total nodes], w0[total edges] (CSR order of
+ * the engine's inputs), K[num_nets] (the gain g(0)), and an optional drive
+ * u[T][total nodes] added to d theta / dt.  The forward pass checkpoints the
+ * state every `segment` steps; backward recomputes each segment and runs one
+ * reverse kernel per step.  All array arguments of lev_adj_forward /
+ * lev_adj_backward are DEVICE pointers (float32) on the engine's device.
+ * The drive array passed to lev_adj_forward must stay valid until
+ * lev_adj_backward returns. */
+typedef struct LevAdjoint LevAdjoint;
+int lev_adj_create(LevAdjoint **out, LevEngine *h, int32_t segment,
+                   int32_t max_steps);
+int lev_adj_destroy(LevAdjoint *a);
+int lev_adj_bytes(const LevAdjoint *a, size_t *bytes);
+/* r_out[T][num_nets]: r after each step; theta_out[T][total nodes] (may be
+ * NULL): phases after each step. */
+int lev_adj_forward(LevAdjoint *a, float dt, int32_t T, const float *omega,
+                    const float *w0_csr, const float *K, const float *drive,
+                    float *r_out, float *theta_out);
+/* dLdr[T][num_nets] (may be NULL), dLdtheta[T][total nodes] (may be NULL);
+ * outputs (each may be NULL): grad_omega[total nodes], grad_w0[total edges]
+ * (CSR order), grad_K[num_nets], grad_drive[T][total nodes]. */
+int lev_adj_backward(LevAdjoint *a, const float *dLdr, const float *dLdtheta,
+                     float *grad_omega, float *grad_w0_csr, float *grad_K,
+                     float *grad_drive);
+/* dL/dtheta(0) of the last backward pass, [total nodes] (device). */
+int lev_adj_grad_theta0(LevAdjoint *a, float *grad_theta0);
+
 /* Self-test of the phase wraps (no reference counterpart; checks this
  * library's division-free evaluation of the wraps of
  * leviathan_kernel.cu:105,146,188).  Runs, on the current device, both

@@ -106,6 +106,12 @@ PROTOTYPES = {
                                  C.POINTER(_i64), C.POINTER(_i32)]),
     "lev_set_variant": (C.c_int, [_P, _i32, _i32]),
     "lev_autotune": (C.c_int, [_P, _f32, _i32, _P, _P]),
+    "lev_adj_create": (C.c_int, [C.POINTER(_P), _P, _i32, _i32]),
+    "lev_adj_destroy": (C.c_int, [_P]),
+    "lev_adj_bytes": (C.c_int, [_P, C.POINTER(C.c_size_t)]),
+    "lev_adj_forward": (C.c_int, [_P, _f32, _i32, _P, _P, _P, _P, _P, _P]),
+    "lev_adj_backward": (C.c_int, [_P, _P, _P, _P, _P, _P, _P]),
+    "lev_adj_grad_theta0": (C.c_int, [_P, _P]),
     "lev_selftest_wraps":(C.c_int, [C.POINTER(C.c_uint64), C.POINTER(C.c_uint64)]),
     "lev_step_noalloc":(C.c_int, [_i32, _i32, _i64, _P, _P, _P, _P, _P, _P, _P,
                                    _P, _P, _P, _P, C.POINTER(LevParams), _f32,

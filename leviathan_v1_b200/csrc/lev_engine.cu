@@ -1434,6 +1434,428 @@ LevEngine *leviathan_engine(LeviathanHandle *handle) {
 }  // extern "C"
 
 // ===========================================================================
+// Adjoint (reverse-mode differentiation through T steps); device code in
+// lev_adjoint.cuh.
+// ===========================================================================
+#include "lev_adjoint.cuh"
+
+namespace lev {
+
+// per-network state set-up: mode 0 init from K (cur 0), mode 1 save g into
+// ck, mode 2 restore g from ck with the segment ring position.
+__global__ void adj_state_kernel(int mode, const NetDesc *nets, NetState *st,
+                                 float *ck_g, const float *K, int num_nets) {
+  for (int n = blockIdx.x * blockDim.x + threadIdx.x; n < num_nets;
+       n += gridDim.x * blockDim.x) {
+    if (mode == 1) {
+      ck_g[n] = st[n].g;
+      continue;
+    }
+    NetState s;
+    s.g = (mode == 0) ? K[n] : ck_g[n];
+    s.r = 0.0f;
+    s.cur = (mode == 0) ? 0 : nets[n].max_delay;
+    s.ticket = 0u;
+    s.t = 0;
+    s.rbuf = 0;
+    s.rpos = 0;
+    st[n] = s;
+  }
+}
+
+}  // namespace lev
+
+struct LevAdjoint {
+  LevEngine *e = nullptr;
+  int C = 50, Tmax = 0, nseg = 0;
+  long long TN = 0, SL = 0;  // total nodes, SELL entries
+  int NN = 0;                // networks
+  std::vector<NetDesc> h_nets;
+  NetDesc *d_nets = nullptr;
+  NetState *d_st = nullptr;
+  long long ring_floats = 0, aux_floats = 0, ckr_floats = 0;
+  long long *d_ck_off = nullptr;
+  float *theta0 = nullptr, *theta_hat0 = nullptr;
+  float *theta = nullptr, *theta_hat = nullptr, *omega = nullptr,
+        *omega_hat = nullptr, *w = nullptr, *ring = nullptr;
+  float2 *partials = nullptr, *bpart = nullptr;
+  unsigned *tickets = nullptr;
+  float *ck_theta = nullptr, *ck_thh = nullptr, *ck_omh = nullptr,
+        *ck_w = nullptr, *ck_ring = nullptr, *ck_g = nullptr;
+  float *w_hist = nullptr, *thh_hist = nullptr;
+  float4 *trace = nullptr;
+  float *lam_th = nullptr, *lam_thh = nullptr, *lam_omh = nullptr,
+        *lam_w = nullptr, *adj_ring = nullptr, *lam_g = nullptr,
+        *grad_omega_acc = nullptr, *grad_theta0 = nullptr;
+  std::vector<void *> allocs;
+  size_t bytes = 0;
+  int last_T = 0;
+  float last_dt = 0.0f;
+  const float *drive = nullptr;
+};
+
+namespace {
+
+template <typename T>
+int adj_alloc(LevAdjoint *a, T **p, long long count) {
+  size_t b = std::max<long long>(count, 1) * sizeof(T);
+  cudaError_t e = cudaMalloc(reinterpret_cast<void **>(p), b);
+  if (e != cudaSuccess) {
+    *p = nullptr;
+    return fail(LEV_ERR_NOMEM, "adjoint: cudaMalloc of " + std::to_string(b) +
+                                   " bytes failed: " + cudaGetErrorString(e));
+  }
+  a->allocs.push_back(*p);
+  a->bytes += b;
+  return LEV_OK;
+}
+
+void adj_free(LevAdjoint *a) {
+  if (!a) return;
+  for (void *p : a->allocs) cudaFree(p);
+  delete a;
+}
+
+AdjFwdArgs adj_fwd_args(LevAdjoint *a, float dt) {
+  AdjFwdArgs f;
+  std::memset(&f, 0, sizeof(f));
+  LevEngine *e = a->e;
+  f.nets = a->d_nets;
+  f.st = a->d_st;
+  f.tiles = e->d_tiles;
+  f.row_ptr = e->d_row_ptr;
+  f.sl_off = e->d_sl_off;
+  f.sl_len = e->d_sl_len;
+  f.sl_cd = e->d_sl_cd;
+  f.w_in = a->w;
+  f.w_out = a->w;
+  f.theta = a->theta;
+  f.theta_hat = a->theta_hat;
+  f.omega = a->omega;
+  f.omega_hat = a->omega_hat;
+  f.ring = a->ring;
+  f.partials = a->partials;
+  f.dt = dt;
+  return f;
+}
+
+int adj_launch_fwd(LevAdjoint *a, const AdjFwdArgs &f) {
+  LevEngine *e = a->e;
+  if (e->math_mode == LEV_MATH_ACCURATE)
+    adj_fwd_kernel<1><<<e->total_tiles, kTile, 0, e->stream>>>(f);
+  else
+    adj_fwd_kernel<0><<<e->total_tiles, kTile, 0, e->stream>>>(f);
+  LEV_TRY_CUDA(cudaGetLastError());
+  return LEV_OK;
+}
+
+int adj_ckpt(LevAdjoint *a, int seg, bool save) {
+  LevEngine *e = a->e;
+  cudaStream_t s = e->stream;
+  const size_t nb = sizeof(float) * a->TN;
+  auto cp = [&](float *ck, float *live, size_t bytes) {
+    return save ? cudaMemcpyAsync(ck, live, bytes, cudaMemcpyDeviceToDevice, s)
+                : cudaMemcpyAsync(live, ck, bytes, cudaMemcpyDeviceToDevice, s);
+  };
+  LEV_TRY_CUDA(cp(a->ck_theta + (size_t)seg * a->TN, a->theta, nb));
+  LEV_TRY_CUDA(cp(a->ck_thh + (size_t)seg * a->TN, a->theta_hat, nb));
+  LEV_TRY_CUDA(cp(a->ck_omh + (size_t)seg * a->TN, a->omega_hat, nb));
+  LEV_TRY_CUDA(cp(a->ck_w + (size_t)seg * a->SL, a->w,
+                  sizeof(float) * std::max<long long>(a->SL, 1)));
+  dim3 grid(64, a->NN);
+  if (save) {
+    adj_state_kernel<<<1, 128, 0, s>>>(1, a->d_nets, a->d_st,
+                                       a->ck_g + (size_t)seg * a->NN, nullptr, a->NN);
+    adj_ring_ckpt_kernel<<<grid, 256, 0, s>>>(0, a->d_nets, a->d_st, a->ring,
+                                              a->ck_ring + (size_t)seg * a->ckr_floats,
+                                              a->d_ck_off, a->NN);
+  } else {
+    adj_ring_ckpt_kernel<<<grid, 256, 0, s>>>(1, a->d_nets, a->d_st, a->ring,
+                                              a->ck_ring + (size_t)seg * a->ckr_floats,
+                                              a->d_ck_off, a->NN);
+    adj_state_kernel<<<1, 128, 0, s>>>(2, a->d_nets, a->d_st,
+                                       a->ck_g + (size_t)seg * a->NN, nullptr, a->NN);
+  }
+  LEV_TRY_CUDA(cudaGetLastError());
+  return LEV_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int lev_adj_create(LevAdjoint **out, LevEngine *e, int32_t segment,
+                   int32_t max_steps) {
+  if (!out || !e) return fail(LEV_ERR_ARG, "null argument");
+  *out = nullptr;
+  if (segment < 1 || max_steps < 1)
+    return fail(LEV_ERR_ARG, "segment and max_steps must be >= 1");
+  DeviceScope ds(e->device);
+  LevAdjoint *a = new LevAdjoint();
+  a->e = e;
+  a->C = segment;
+  a->Tmax = max_steps;
+  a->nseg = (max_steps + segment - 1) / segment;
+  a->TN = e->total_nodes;
+  a->SL = e->sl_total;
+  a->NN = e->num_nets;
+  a->h_nets = e->h_nets;
+  std::vector<long long> ck_off(a->NN);
+  for (int n = 0; n < a->NN; ++n) {
+    NetDesc &d = a->h_nets[n];
+    d.bsi = segment + d.max_delay + 2;
+    d.ring_off = a->ring_floats;
+    d.aux_off = a->aux_floats;
+    a->ring_floats += (long long)d.bsi * d.Np;
+    a->aux_floats += (long long)(d.max_delay + 2) * d.Np;
+    ck_off[n] = a->ckr_floats;
+    a->ckr_floats += (long long)(d.max_delay + 1) * d.N;
+    if ((unsigned long long)d.bsi * (unsigned long long)d.Np >= (1ull << 32)) {
+      delete a;
+      return fail(LEV_ERR_ARG, "adjoint: (segment + max_delay + 2) * N must be below 2^32");
+    }
+  }
+  const long long TN = a->TN, SL = a->SL, NN = a->NN;
+  const long long S = a->nseg, C = a->C;
+  int rc = LEV_OK;
+#define A(ptr, n) \
+  if (rc == LEV_OK) rc = adj_alloc(a, &(ptr), (n));
+  A(a->d_nets, NN);
+  A(a->d_st, NN);
+  A(a->d_ck_off, NN);
+  A(a->theta0, TN); A(a->theta_hat0, TN);
+  A(a->theta, TN); A(a->theta_hat, TN); A(a->omega, TN); A(a->omega_hat, TN);
+  A(a->w, SL);
+  A(a->ring, a->ring_floats);
+  A(a->partials, e->total_tiles);
+  A(a->bpart, e->total_tiles);
+  A(a->tickets, NN);
+  A(a->ck_theta, S * TN); A(a->ck_thh, S * TN); A(a->ck_omh, S * TN);
+  A(a->ck_w, S * SL);
+  A(a->ck_ring, S * a->ckr_floats);
+  A(a->ck_g, S * NN);
+  A(a->w_hist, (C + 1) * SL);
+  A(a->thh_hist, C * TN);
+  A(a->trace, C * NN);
+  A(a->lam_th, TN); A(a->lam_thh, TN); A(a->lam_omh, TN);
+  A(a->lam_w, SL);
+  A(a->adj_ring, a->aux_floats);
+  A(a->lam_g, NN);
+  A(a->grad_omega_acc, TN);
+  A(a->grad_theta0, TN);
+#undef A
+  if (rc != LEV_OK) {
+    std::string msg = g_last_error;
+    adj_free(a);
+    return fail(rc, msg);
+  }
+  cudaStream_t s = e->stream;
+  cudaError_t ce = cudaMemcpyAsync(a->d_nets, a->h_nets.data(), sizeof(NetDesc) * NN,
+                                   cudaMemcpyHostToDevice, s);
+  if (ce == cudaSuccess)
+    ce = cudaMemcpyAsync(a->d_ck_off, ck_off.data(), sizeof(long long) * NN,
+                         cudaMemcpyHostToDevice, s);
+  // initial conditions: the engine's current phases and predictor phases
+  if (ce == cudaSuccess)
+    ce = cudaMemcpyAsync(a->theta0, e->d_theta, sizeof(float) * TN,
+                         cudaMemcpyDeviceToDevice, s);
+  if (ce == cudaSuccess)
+    ce = cudaMemcpyAsync(a->theta_hat0, e->d_theta_hat, sizeof(float) * TN,
+                         cudaMemcpyDeviceToDevice, s);
+  if (ce == cudaSuccess) ce = cudaMemsetAsync(a->tickets, 0, sizeof(unsigned) * NN, s);
+  if (ce == cudaSuccess) ce = cudaStreamSynchronize(s);
+  if (ce != cudaSuccess) {
+    adj_free(a);
+    return fail(LEV_ERR_CUDA, std::string("adjoint set-up: ") + cudaGetErrorString(ce));
+  }
+  *out = a;
+  return LEV_OK;
+}
+
+int lev_adj_destroy(LevAdjoint *a) {
+  if (!a) return LEV_OK;
+  DeviceScope ds(a->e->device);
+  cudaStreamSynchronize(a->e->stream);
+  adj_free(a);
+  return LEV_OK;
+}
+
+int lev_adj_bytes(const LevAdjoint *a, size_t *bytes) {
+  if (!a || !bytes) return fail(LEV_ERR_ARG, "null argument");
+  *bytes = a->bytes;
+  return LEV_OK;
+}
+
+int lev_adj_forward(LevAdjoint *a, float dt, int32_t T, const float *omega,
+                    const float *w0_csr, const float *K, const float *drive,
+                    float *r_out, float *theta_out) {
+  if (!a || !omega || !w0_csr || !K || !r_out)
+    return fail(LEV_ERR_ARG, "null argument");
+  if (T < 1 || T > a->Tmax)
+    return fail(LEV_ERR_ARG, "T must be in [1, max_steps]");
+  if (!std::isfinite(dt)) return fail(LEV_ERR_ARG, "dt is not finite");
+  LevEngine *e = a->e;
+  DeviceScope ds(e->device);
+  cudaStream_t s = e->stream;
+  const size_t nb = sizeof(float) * a->TN;
+  LEV_TRY_CUDA(cudaMemcpyAsync(a->theta, a->theta0, nb, cudaMemcpyDeviceToDevice, s));
+  LEV_TRY_CUDA(cudaMemcpyAsync(a->theta_hat, a->theta_hat0, nb, cudaMemcpyDeviceToDevice, s));
+  LEV_TRY_CUDA(cudaMemcpyAsync(a->omega, omega, nb, cudaMemcpyDeviceToDevice, s));
+  // omega_hat starts as omega (leviathan_kernel.cu:350)
+  LEV_TRY_CUDA(cudaMemcpyAsync(a->omega_hat, omega, nb, cudaMemcpyDeviceToDevice, s));
+  LEV_TRY_CUDA(cudaMemsetAsync(a->w, 0, sizeof(float) * std::max<long long>(a->SL, 1), s));
+  for (int n = 0; n < a->NN; ++n) {
+    const NetDesc &d = a->h_nets[n];
+    if (e->net_E[n] == 0) continue;
+    int blocks = (int)std::min<long long>((d.N + 255) / 256, 148LL * 16);
+    sell_convert_kernel<<<blocks, 256, 0, s>>>(
+        1, e->d_row_ptr + d.rp_off, d.N, d.slice_base, e->d_sl_off, nullptr,
+        nullptr, const_cast<float *>(w0_csr) + d.edge_off, e->d_sl_cd, a->w,
+        d.max_delay, nullptr);
+    const long long total = (long long)d.bsi * d.N;
+    int fb = (int)std::min<long long>((total + 255) / 256, 148LL * 16);
+    ring_fill_kernel<<<fb, 256, 0, s>>>(a->theta0 + d.node_off, a->ring + d.ring_off,
+                                       d.N, d.Np, d.bsi);
+  }
+  adj_state_kernel<<<1, 128, 0, s>>>(0, a->d_nets, a->d_st, nullptr, K, a->NN);
+  LEV_TRY_CUDA(cudaGetLastError());
+  AdjFwdArgs f = adj_fwd_args(a, dt);
+  f.drive = nullptr;
+  for (int t = 0; t < T; ++t) {
+    if (t % a->C == 0) {
+      int rc = adj_ckpt(a, t / a->C, true);
+      if (rc != LEV_OK) return rc;
+    }
+    f.drive = drive ? drive + (size_t)t * a->TN : nullptr;
+    f.r_out = r_out + (size_t)t * a->NN;
+    f.theta_out = theta_out ? theta_out + (size_t)t * a->TN : nullptr;
+    int rc = adj_launch_fwd(a, f);
+    if (rc != LEV_OK) return rc;
+  }
+  LEV_TRY_CUDA(cudaStreamSynchronize(s));
+  a->last_T = T;
+  a->last_dt = dt;
+  a->drive = drive;
+  return LEV_OK;
+}
+
+int lev_adj_backward(LevAdjoint *a, const float *dLdr, const float *dLdtheta,
+                     float *grad_omega, float *grad_w0_csr, float *grad_K,
+                     float *grad_drive) {
+  if (!a) return fail(LEV_ERR_ARG, "null handle");
+  if (a->last_T < 1) return fail(LEV_ERR_STATE, "lev_adj_backward before lev_adj_forward");
+  LevEngine *e = a->e;
+  DeviceScope ds(e->device);
+  cudaStream_t s = e->stream;
+  const int T = a->last_T;
+  const float dt = a->last_dt;
+  const size_t nb = sizeof(float) * a->TN;
+  const size_t wb = sizeof(float) * std::max<long long>(a->SL, 1);
+  LEV_TRY_CUDA(cudaMemsetAsync(a->lam_th, 0, nb, s));
+  LEV_TRY_CUDA(cudaMemsetAsync(a->lam_thh, 0, nb, s));
+  LEV_TRY_CUDA(cudaMemsetAsync(a->lam_omh, 0, nb, s));
+  LEV_TRY_CUDA(cudaMemsetAsync(a->grad_omega_acc, 0, nb, s));
+  LEV_TRY_CUDA(cudaMemsetAsync(a->lam_w, 0, wb, s));
+  LEV_TRY_CUDA(cudaMemsetAsync(a->adj_ring, 0, sizeof(float) * std::max<long long>(a->aux_floats, 1), s));
+  LEV_TRY_CUDA(cudaMemsetAsync(a->lam_g, 0, sizeof(float) * a->NN, s));
+  LEV_TRY_CUDA(cudaMemsetAsync(a->tickets, 0, sizeof(unsigned) * a->NN, s));
+  const int nseg = (T + a->C - 1) / a->C;
+  const int mode = (e->math_mode == LEV_MATH_ACCURATE) ? 1 : 0;
+  for (int seg = nseg - 1; seg >= 0; --seg) {
+    const int s0 = seg * a->C, s1 = std::min(T, s0 + a->C);
+    // recompute the segment forward, recording what the reverse steps need
+    int rc = adj_ckpt(a, seg, false);
+    if (rc != LEV_OK) return rc;
+    LEV_TRY_CUDA(cudaMemcpyAsync(a->w_hist, a->w, wb, cudaMemcpyDeviceToDevice, s));
+    AdjFwdArgs f = adj_fwd_args(a, dt);
+    for (int t = s0; t < s1; ++t) {
+      const int k = t - s0;
+      f.w_in = a->w_hist + (size_t)k * a->SL;
+      f.w_out = a->w_hist + (size_t)(k + 1) * a->SL;
+      f.thh_rec = a->thh_hist + (size_t)k * a->TN;
+      f.trace = a->trace + (size_t)k * a->NN;
+      f.drive = a->drive ? a->drive + (size_t)t * a->TN : nullptr;
+      f.r_out = nullptr;
+      f.theta_out = nullptr;
+      rc = adj_launch_fwd(a, f);
+      if (rc != LEV_OK) return rc;
+    }
+    // reverse steps
+    AdjBwdArgs b;
+    std::memset(&b, 0, sizeof(b));
+    b.nets = a->d_nets;
+    b.tiles = e->d_tiles;
+    b.row_ptr = e->d_row_ptr;
+    b.sl_off = e->d_sl_off;
+    b.sl_len = e->d_sl_len;
+    b.sl_cd = e->d_sl_cd;
+    b.H = a->ring;
+    b.lam_th = a->lam_th;
+    b.lam_thh = a->lam_thh;
+    b.lam_omh = a->lam_omh;
+    b.lam_w = a->lam_w;
+    b.adj_ring = a->adj_ring;
+    b.lam_g = a->lam_g;
+    b.grad_omega = a->grad_omega_acc;
+    b.partials = a->bpart;
+    b.tickets = a->tickets;
+    b.seg_start = s0;
+    b.dt = dt;
+    for (int t = s1 - 1; t >= s0; --t) {
+      const int k = t - s0;
+      b.s = t;
+      b.w_s = a->w_hist + (size_t)k * a->SL;
+      b.thh_s = a->thh_hist + (size_t)k * a->TN;
+      b.trace = a->trace + (size_t)k * a->NN;
+      b.dLdr = dLdr ? dLdr + (size_t)t * a->NN : nullptr;
+      b.dLdth = dLdtheta ? dLdtheta + (size_t)t * a->TN : nullptr;
+      b.grad_drive = grad_drive ? grad_drive + (size_t)t * a->TN : nullptr;
+      if (mode)
+        adj_bwd_kernel<1><<<e->total_tiles, kTile, 0, s>>>(b);
+      else
+        adj_bwd_kernel<0><<<e->total_tiles, kTile, 0, s>>>(b);
+      LEV_TRY_CUDA(cudaGetLastError());
+    }
+  }
+  // gradients
+  dim3 grid(64, a->NN);
+  adj_finalize_kernel<<<grid, 256, 0, s>>>(a->d_nets, a->NN, a->lam_th, a->adj_ring,
+                                           a->grad_theta0);
+  if (grad_omega) {
+    // omega enters directly and through omega_hat(0) = omega
+    LEV_TRY_CUDA(cudaMemcpyAsync(grad_omega, a->grad_omega_acc, nb, cudaMemcpyDeviceToDevice, s));
+    add_kernel<<<148, 256, 0, s>>>(grad_omega, a->lam_omh, a->TN);
+  }
+  if (grad_w0_csr) {
+    for (int n = 0; n < a->NN; ++n) {
+      const NetDesc &d = a->h_nets[n];
+      if (e->net_E[n] == 0) continue;
+      int blocks = (int)std::min<long long>((d.N + 255) / 256, 148LL * 16);
+      sell_convert_kernel<<<blocks, 256, 0, s>>>(
+          2, e->d_row_ptr + d.rp_off, d.N, d.slice_base, e->d_sl_off, nullptr, nullptr,
+          grad_w0_csr + d.edge_off, e->d_sl_cd, a->lam_w, d.max_delay, nullptr);
+    }
+  }
+  if (grad_K)
+    LEV_TRY_CUDA(cudaMemcpyAsync(grad_K, a->lam_g, sizeof(float) * a->NN,
+                                 cudaMemcpyDeviceToDevice, s));
+  LEV_TRY_CUDA(cudaGetLastError());
+  LEV_TRY_CUDA(cudaStreamSynchronize(s));
+  return LEV_OK;
+}
+
+int lev_adj_grad_theta0(LevAdjoint *a, float *grad_theta0) {
+  if (!a || !grad_theta0) return fail(LEV_ERR_ARG, "null argument");
+  DeviceScope ds(a->e->device);
+  LEV_TRY_CUDA(cudaMemcpyAsync(grad_theta0, a->grad_theta0, sizeof(float) * a->TN,
+                               cudaMemcpyDeviceToDevice, a->e->stream));
+  LEV_TRY_CUDA(cudaStreamSynchronize(a->e->stream));
+  return LEV_OK;
+}
+
+}  // extern "C"
+
+// ===========================================================================
 // Allocation-free step: lev_step_noalloc
 //
 // For callers that cannot call cudaMalloc: code whose device memory is owned

@@ -61,6 +61,7 @@ struct NetDesc {
   long long ring_off;  // first float of the ring (multiple of 32)
   long long rp_off;    // first entry of the local row_ptr (N+1 entries)
   long long slice_base;  // first SELL slice of this network
+  long long aux_off;     // first float of the network's adjoint ring (adjoint only)
   int N;
   int Np;         // ring row pitch
   int bsi;        // ring slots = max_delay + 2
