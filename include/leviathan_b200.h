@@ -276,6 +276,21 @@ int lev_adj_backward(LevAdjoint *a, const float *dLdr, const float *dLdtheta,
 /* dL/dtheta(0) of the last backward pass, [total nodes] (device). */
 int lev_adj_grad_theta0(LevAdjoint *a, float *grad_theta0);
 
+/* Reservoir terms fused into the adjoint's forward and reverse kernels
+ * (device pointers, kept until replaced; NULL pairs disable a term):
+ *   drive    u_i(t) = win[i] * x[t][network of i]      (win [total nodes],
+ *            x [T][num_nets]) added to d theta_i / dt;
+ *   readout  y[t][n] = sum_{i in n} ra[i] cos theta_i(t+1) + rb[i] sin theta_i(t+1)
+ *            written to y_out[T][num_nets] by lev_adj_forward.
+ * Set before lev_adj_forward.  For the backward pass set dL/dy [T][num_nets]
+ * and the accumulators grad_win, grad_ra, grad_rb [total nodes] (zeroed by
+ * lev_adj_backward, each may be NULL) with lev_adj_set_reservoir_grads. */
+int lev_adj_set_reservoir(LevAdjoint *a, const float *win, const float *x,
+                          const float *ra, const float *rb, float *y_out);
+int lev_adj_set_reservoir_grads(LevAdjoint *a, const float *dLdy,
+                                float *grad_win, float *grad_ra,
+                                float *grad_rb);
+
 /* Self-test of the phase wraps (no reference counterpart; checks this
  * library's division-free evaluation of the wraps of
  * leviathan_kernel.cu:105,146,188).  Runs, on the current device, both

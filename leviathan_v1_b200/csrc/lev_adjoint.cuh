@@ -58,6 +58,14 @@ struct AdjFwdArgs {
   float4 *trace;       // per network (g used, r, sum cos, sum sin), or null
   float *r_out;        // per network r after the step, or null
   float *theta_out;    // theta after the step [total nodes], or null
+  // reservoir: drive u_i = win_i * xin[network]; readout
+  // y[network] = sum_i ra_i cos theta_i + rb_i sin theta_i (after the step)
+  const float *win;    // [total nodes] or null
+  const float *xin;    // [num_nets] input of this step
+  const float *ra;     // [total nodes] or null
+  const float *rb;
+  float *ro_partials;  // per tile
+  float *y_out;        // per network, or null
   float dt;
 };
 
@@ -67,6 +75,7 @@ template <int MATH>
 __global__ void __launch_bounds__(kTile, 3) adj_fwd_kernel(const AdjFwdArgs a) {
   __shared__ float s_rc[32];
   __shared__ float s_rs[32];
+  __shared__ float s_ry[32];
   __shared__ int s_last;
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   const int2 tile = a.tiles[blockIdx.x];
@@ -142,13 +151,17 @@ __global__ void __launch_bounds__(kTile, 3) adj_fwd_kernel(const AdjFwdArgs a) {
 
   int nxt = cur + 1;
   if (nxt == bsi) nxt = 0;
-  float my_cos = 0.0f, my_sin = 0.0f;
+  float my_cos = 0.0f, my_sin = 0.0f, my_y = 0.0f;
   if (live) {
     float inc;
-    if (a.drive)
-      inc = dt * (a.omega[gi] + g * local_sum - nd.alpha * eps + a.drive[gi]);
-    else
+    if (a.drive || a.win) {
+      float u = 0.0f;
+      if (a.drive) u += a.drive[gi];
+      if (a.win) u += a.win[gi] * a.xin[tile.x];
+      inc = dt * (a.omega[gi] + g * local_sum - nd.alpha * eps + u);
+    } else {
       inc = dt * (a.omega[gi] + g * local_sum - nd.alpha * eps);
+    }
     float x = th + inc;
     x = wrap_0_2pi(x);
     if (!isfinite(x)) x = 0.0f;
@@ -156,28 +169,34 @@ __global__ void __launch_bounds__(kTile, 3) adj_fwd_kernel(const AdjFwdArgs a) {
     if (a.theta_out) a.theta_out[gi] = x;
     a.ring[nd.ring_off + (long long)nxt * Np + row] = x;
     lev_sincos<MATH>(x, &my_sin, &my_cos);
+    if (a.ra) my_y = a.ra[gi] * my_cos + a.rb[gi] * my_sin;
   }
   const unsigned mask = 0xffffffffu;
 #pragma unroll
   for (int off = 16; off > 0; off /= 2) {
     my_cos += __shfl_down_sync(mask, my_cos, off);
     my_sin += __shfl_down_sync(mask, my_sin, off);
+    my_y += __shfl_down_sync(mask, my_y, off);
   }
   if (lane == 0) {
     s_rc[warp] = my_cos;
     s_rs[warp] = my_sin;
+    s_ry[warp] = my_y;
   }
   __syncthreads();
   if (warp == 0) {
     my_cos = (lane < (kTile / 32)) ? s_rc[lane] : 0.0f;
     my_sin = (lane < (kTile / 32)) ? s_rs[lane] : 0.0f;
+    my_y = (lane < (kTile / 32)) ? s_ry[lane] : 0.0f;
 #pragma unroll
     for (int off = 16; off > 0; off /= 2) {
       my_cos += __shfl_down_sync(mask, my_cos, off);
       my_sin += __shfl_down_sync(mask, my_sin, off);
+      my_y += __shfl_down_sync(mask, my_y, off);
     }
     if (lane == 0) {
       a.partials[nd.part_off + row0 / kTile] = make_float2(my_cos, my_sin);
+      if (a.ra) a.ro_partials[nd.part_off + row0 / kTile] = my_y;
       __threadfence();
       const unsigned prev = atomicAdd(&ns->ticket, 1u);
       s_last = (prev == (unsigned)(nd.ntiles - 1));
@@ -205,6 +224,11 @@ __global__ void __launch_bounds__(kTile, 3) adj_fwd_kernel(const AdjFwdArgs a) {
       const float gn = nd.ctrl ? gain_controller(g, r, dt, nd) : g;
       if (a.trace) a.trace[tile.x] = make_float4(g, r, sum_cos, sum_sin);
       if (a.r_out) a.r_out[tile.x] = r;
+      if (a.ra && a.y_out) {
+        float y = 0.0f;
+        for (int k = 0; k < nd.ntiles; ++k) y += __ldcg(a.ro_partials + nd.part_off + k);
+        a.y_out[tile.x] = y;
+      }
       ns->g = gn;
       ns->r = r;
       ns->cur = nxt;
@@ -237,6 +261,15 @@ struct AdjBwdArgs {
   float *grad_drive;   // [total nodes] for step s, or null
   float2 *partials;    // per tile (lam_g partial, unused)
   unsigned *tickets;   // per network
+  // reservoir terms (see AdjFwdArgs); all may be null
+  const float *win;
+  const float *xin;    // [num_nets] input of step s
+  float *grad_win;     // accumulated
+  const float *ra;
+  const float *rb;
+  const float *dLdy;   // [num_nets] dL/dy(s+1)
+  float *grad_ra;      // accumulated
+  float *grad_rb;
   long long s;         // step being reversed (absolute)
   long long seg_start;
   float dt;
@@ -290,16 +323,21 @@ __global__ void __launch_bounds__(kTile, 3) adj_bwd_kernel(const AdjBwdArgs a) {
     float* slot_next = AR + (long long)as_next * Np + row;
     lt1 = a.lam_th[gi] + *slot_next;
     *slot_next = 0.0f;
-    if (r1 > 0.0f) {
-      float sn, cs;
-      sincosf(th1, &sn, &cs);
-      lt1 += lam_r * (Sm * cs - Cm * sn) * invN / r1;
-    }
+    float sn, cs;
+    sincosf(th1, &sn, &cs);
+    if (r1 > 0.0f) lt1 += lam_r * (Sm * cs - Cm * sn) * invN / r1;
     if (a.dLdth) lt1 += a.dLdth[gi];
+    if (a.dLdy) {  // readout y = sum ra cos theta + rb sin theta
+      const float gy = a.dLdy[tile.x];
+      lt1 += gy * (a.rb[gi] * cs - a.ra[gi] * sn);
+      a.grad_ra[gi] += gy * cs;
+      a.grad_rb[gi] += gy * sn;
+    }
     // (B) integrate
     lam_S = lt1 * dt * g_s;
     a.grad_omega[gi] += lt1 * dt;
     if (a.grad_drive) a.grad_drive[gi] = lt1 * dt;
+    if (a.grad_win) a.grad_win[gi] += lt1 * dt * a.xin[tile.x];
     // prep recompute
     th = H[(long long)hs * Np + row];
     diff = wrap_pm_pi(th - a.thh_s[gi]);

@@ -1492,6 +1492,13 @@ struct LevAdjoint {
   int last_T = 0;
   float last_dt = 0.0f;
   const float *drive = nullptr;
+  // reservoir (fused drive win * x and cos/sin readout), all device pointers
+  const float *res_win = nullptr, *res_x = nullptr, *res_ra = nullptr,
+              *res_rb = nullptr;
+  float *res_y = nullptr;
+  const float *res_dLdy = nullptr;
+  float *res_gwin = nullptr, *res_gra = nullptr, *res_grb = nullptr;
+  float *ro_partials = nullptr;
 };
 
 namespace {
@@ -1629,6 +1636,7 @@ int lev_adj_create(LevAdjoint **out, LevEngine *e, int32_t segment,
   A(a->ring, a->ring_floats);
   A(a->partials, e->total_tiles);
   A(a->bpart, e->total_tiles);
+  A(a->ro_partials, e->total_tiles);
   A(a->tickets, NN);
   A(a->ck_theta, S * TN); A(a->ck_thh, S * TN); A(a->ck_omh, S * TN);
   A(a->ck_w, S * SL);
@@ -1729,6 +1737,16 @@ int lev_adj_forward(LevAdjoint *a, float dt, int32_t T, const float *omega,
     f.drive = drive ? drive + (size_t)t * a->TN : nullptr;
     f.r_out = r_out + (size_t)t * a->NN;
     f.theta_out = theta_out ? theta_out + (size_t)t * a->TN : nullptr;
+    if (a->res_win) {
+      f.win = a->res_win;
+      f.xin = a->res_x + (size_t)t * a->NN;
+    }
+    if (a->res_ra) {
+      f.ra = a->res_ra;
+      f.rb = a->res_rb;
+      f.ro_partials = a->ro_partials;
+      f.y_out = a->res_y ? a->res_y + (size_t)t * a->NN : nullptr;
+    }
     int rc = adj_launch_fwd(a, f);
     if (rc != LEV_OK) return rc;
   }
@@ -1759,6 +1777,9 @@ int lev_adj_backward(LevAdjoint *a, const float *dLdr, const float *dLdtheta,
   LEV_TRY_CUDA(cudaMemsetAsync(a->adj_ring, 0, sizeof(float) * std::max<long long>(a->aux_floats, 1), s));
   LEV_TRY_CUDA(cudaMemsetAsync(a->lam_g, 0, sizeof(float) * a->NN, s));
   LEV_TRY_CUDA(cudaMemsetAsync(a->tickets, 0, sizeof(unsigned) * a->NN, s));
+  if (a->res_gwin) LEV_TRY_CUDA(cudaMemsetAsync(a->res_gwin, 0, nb, s));
+  if (a->res_gra) LEV_TRY_CUDA(cudaMemsetAsync(a->res_gra, 0, nb, s));
+  if (a->res_grb) LEV_TRY_CUDA(cudaMemsetAsync(a->res_grb, 0, nb, s));
   const int nseg = (T + a->C - 1) / a->C;
   const int mode = (e->math_mode == LEV_MATH_ACCURATE) ? 1 : 0;
   for (int seg = nseg - 1; seg >= 0; --seg) {
@@ -1777,6 +1798,10 @@ int lev_adj_backward(LevAdjoint *a, const float *dLdr, const float *dLdtheta,
       f.drive = a->drive ? a->drive + (size_t)t * a->TN : nullptr;
       f.r_out = nullptr;
       f.theta_out = nullptr;
+      if (a->res_win) {
+        f.win = a->res_win;
+        f.xin = a->res_x + (size_t)t * a->NN;
+      }
       rc = adj_launch_fwd(a, f);
       if (rc != LEV_OK) return rc;
     }
@@ -1810,6 +1835,18 @@ int lev_adj_backward(LevAdjoint *a, const float *dLdr, const float *dLdtheta,
       b.dLdr = dLdr ? dLdr + (size_t)t * a->NN : nullptr;
       b.dLdth = dLdtheta ? dLdtheta + (size_t)t * a->TN : nullptr;
       b.grad_drive = grad_drive ? grad_drive + (size_t)t * a->TN : nullptr;
+      if (a->res_win) {
+        b.win = a->res_win;
+        b.xin = a->res_x + (size_t)t * a->NN;
+        b.grad_win = a->res_gwin;
+      }
+      if (a->res_ra && a->res_dLdy) {
+        b.ra = a->res_ra;
+        b.rb = a->res_rb;
+        b.dLdy = a->res_dLdy + (size_t)t * a->NN;
+        b.grad_ra = a->res_gra;
+        b.grad_rb = a->res_grb;
+      }
       if (mode)
         adj_bwd_kernel<1><<<e->total_tiles, kTile, 0, s>>>(b);
       else
@@ -1841,6 +1878,36 @@ int lev_adj_backward(LevAdjoint *a, const float *dLdr, const float *dLdtheta,
                                  cudaMemcpyDeviceToDevice, s));
   LEV_TRY_CUDA(cudaGetLastError());
   LEV_TRY_CUDA(cudaStreamSynchronize(s));
+  return LEV_OK;
+}
+
+int lev_adj_set_reservoir(LevAdjoint *a, const float *win, const float *x,
+                          const float *ra, const float *rb, float *y_out) {
+  if (!a) return fail(LEV_ERR_ARG, "null handle");
+  if ((win == nullptr) != (x == nullptr))
+    return fail(LEV_ERR_ARG, "win and x must be given together");
+  if ((ra == nullptr) != (rb == nullptr))
+    return fail(LEV_ERR_ARG, "ra and rb must be given together");
+  a->res_win = win;
+  a->res_x = x;
+  a->res_ra = ra;
+  a->res_rb = rb;
+  a->res_y = y_out;
+  return LEV_OK;
+}
+
+int lev_adj_set_reservoir_grads(LevAdjoint *a, const float *dLdy,
+                                float *grad_win, float *grad_ra,
+                                float *grad_rb) {
+  if (!a) return fail(LEV_ERR_ARG, "null handle");
+  if (grad_win && !a->res_win)
+    return fail(LEV_ERR_STATE, "no input weights set (lev_adj_set_reservoir)");
+  if ((dLdy || grad_ra || grad_rb) && !a->res_ra)
+    return fail(LEV_ERR_STATE, "no readout set (lev_adj_set_reservoir)");
+  a->res_dLdy = dLdy;
+  a->res_gwin = grad_win;
+  a->res_gra = grad_ra;
+  a->res_grb = grad_rb;
   return LEV_OK;
 }
 
