@@ -27,6 +27,7 @@ from __future__ import annotations
 
 import argparse
 import json
+import math
 import os
 import statistics
 import subprocess
@@ -309,6 +310,114 @@ def run_batched(args, rank, world, plain_value):
 
 
 # ---------------------------------------------------------------------------
+# adjoint (N=1e4, k=20, 2000 steps, checkpoint every 50) and differentiable
+# reservoir (batch 64 x N=5e4, k=20, 1000 steps)
+# ---------------------------------------------------------------------------
+def _cuda_time(fn):
+    import torch
+
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    out = fn()
+    torch.cuda.synchronize()
+    return out, time.perf_counter() - t0
+
+
+def run_adjoint(args):
+    import torch
+
+    from leviathan_v1_b200 import LeviathanEngine
+    from leviathan_v1_b200.adjoint import Adjoint, simulate
+    from leviathan_v1_b200.graphs import config_adjoint
+
+    T, C = args.adjoint_steps, 50
+    net = config_adjoint(0)
+    eng = LeviathanEngine(*net.engine_args(), math_mode="accurate")
+    adj = Adjoint(eng, segment=C, max_steps=T)
+    om = torch.tensor(net.omega, device="cuda", requires_grad=True)
+    w0 = torch.tensor(net.weights, device="cuda", requires_grad=True)
+    K = torch.full((1,), 1.5, device="cuda", requires_grad=True)
+    t = torch.arange(1, T + 1, device="cuda", dtype=torch.float32)
+    tgt = 0.5 + 0.2 * torch.sin(2 * math.pi * t / 400.0)
+
+    def fwd():
+        return simulate(adj, om, w0, K, T, DT)[:, 0]
+
+    def fwd_bwd():
+        r = fwd()
+        L = torch.mean((r - tgt) ** 2)
+        L.backward()
+        return L
+
+    fwd_bwd()  # warm-up
+    om.grad = w0.grad = K.grad = None
+    _, t_f = _cuda_time(fwd)
+    L, t_fb = _cuda_time(fwd_bwd)
+    plain = LeviathanEngine(*net.engine_args(), math_mode="accurate")
+    plain.step_n(DT, 50)
+    _, t_plain = _cuda_time(lambda: plain.step_n(DT, T))
+    plain.close()
+    out = {"workload": "N=1e4, k=20, delays U[1,50], T=2000 steps, checkpoint every 50, "
+                       "loss = MSE(r, 0.5 + 0.2 sin(2 pi t/400)), grads w.r.t. omega, w, K",
+           "N": net.N, "E": net.E, "T": T, "segment": C,
+           "fwd_s": t_f, "fwd_bwd_s": t_fb, "fwd_bwd_over_fwd": t_fb / t_f,
+           "fwd_edge_updates_per_s": net.E * T / t_f,
+           "plain_engine_edge_updates_per_s": net.E * T / t_plain,
+           "loss": float(L.detach()), "grad_norms": {
+               "omega": float(om.grad.norm()), "w": float(w0.grad.norm()),
+               "K": float(K.grad.abs().sum())},
+           "device_bytes": adj.device_bytes,
+           "gradient_check": "rel. error <= 1e-3 vs FP64 autograd and FP64 finite "
+                             "differences at N=200, k=8, 100 steps (tests/test_adjoint_gpu.py)"}
+    adj.close()
+    eng.close()
+    return out
+
+
+def run_reservoir(args):
+    import torch
+
+    from leviathan_v1_b200.graphs import config_reservoir
+    from leviathan_v1_b200.reservoir import DifferentiableReservoir, make_inputs
+
+    B, T = 64, args.reservoir_steps
+    net = config_reservoir(0)
+    model = DifferentiableReservoir(net, B, n_input=256, T=T, segment=50, seed=0)
+    x = torch.tensor(make_inputs(B, T, seed=0), device="cuda")
+
+    def fwd():
+        with torch.no_grad():
+            return model(x, DT)
+
+    def fwd_bwd():
+        y, r = model(x, DT)
+        L = model.loss(y, x, 10)
+        L.backward()
+        return L
+
+    fwd_bwd()  # warm-up
+    model.zero_grad()
+    _, t_f = _cuda_time(fwd)
+    L, t_fb = _cuda_time(fwd_bwd)
+    E_tot = net.E * B
+    out = {"workload": "batch 64 x (N=5e4, k=20, delays U[1,50]), T=1000, 256 input nodes, "
+                       "readout on cos/sin of all phases predicts x(t+10); grads w.r.t. W_in, "
+                       "omega, readout",
+           "batch": B, "N": net.N, "E_per_copy": net.E, "T": T,
+           "fwd_s": t_f, "fwd_bwd_s": t_fb, "fwd_bwd_over_fwd": t_fb / t_f,
+           "fwd_edge_updates_per_s": E_tot * T / t_f,
+           "loss": float(L.detach()),
+           "grad_norms": {"w_in": float(model.w_in.grad.norm()),
+                          "omega": float(model.omega.grad.norm()),
+                          "readout": float(model.read_a.grad.norm() + model.read_b.grad.norm())},
+           "device_bytes": model.adj.device_bytes,
+           "gradient_check": "rel. error <= 1e-3 vs FP64 autograd at N=200, batch 3, 60 "
+                             "steps (tests/test_reservoir_gpu.py)"}
+    model.close()
+    return out
+
+
+# ---------------------------------------------------------------------------
 # our engine
 # ---------------------------------------------------------------------------
 def run_ours(args, rank, world, local):
@@ -396,6 +505,9 @@ def run_ours(args, rank, world, local):
     }
     if not args.no_batched:
         line["batched"] = run_batched(args, rank, world, value)
+    if rank == 0 and not args.no_adjoint:
+        line["adjoint"] = run_adjoint(args)
+        line["reservoir"] = run_reservoir(args)
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline(net, budget_s=args.cpu_budget)
     if rank == 0 and not args.no_fp64_check:
@@ -475,6 +587,9 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-fp64-check", action="store_true")
     ap.add_argument("--no-batched", action="store_true")
+    ap.add_argument("--no-adjoint", action="store_true")
+    ap.add_argument("--adjoint-steps", type=int, default=2000)
+    ap.add_argument("--reservoir-steps", type=int, default=1000)
     ap.add_argument("--batched-steps", type=int, default=200)
     args = ap.parse_args()
     if args.warmup < 3:

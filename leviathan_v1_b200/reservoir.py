@@ -96,8 +96,11 @@ class DifferentiableReservoir(torch.nn.Module):
                                                     dtype=torch.float32, device=device))
         self.omega = torch.nn.Parameter(torch.tensor(net.omega, device=device))
         self.register_buffer("w0", torch.tensor(net.weights, device=device))
-        self.read_a = torch.nn.Parameter(torch.zeros(self.N, device=device))
-        self.read_b = torch.nn.Parameter(torch.zeros(self.N, device=device))
+        # small random readout: with an all-zero readout no gradient reaches
+        # the dynamics (W_in, omega) until the readout itself has moved
+        ro = rng.normal(0.0, 1.0 / math.sqrt(2 * self.N), (2, self.N))
+        self.read_a = torch.nn.Parameter(torch.tensor(ro[0], dtype=torch.float32, device=device))
+        self.read_b = torch.nn.Parameter(torch.tensor(ro[1], dtype=torch.float32, device=device))
         self.read_c = torch.nn.Parameter(torch.zeros(1, device=device))
         self.K = float((params or {}).get("g", 1.5))
 
