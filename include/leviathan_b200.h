@@ -232,6 +232,18 @@ int lev_class_info(const LevEngine *h, int32_t c, int32_t *ntiles,
                    float *mean_slice_len, int64_t *edges, int32_t *variant);
 int lev_set_variant(LevEngine *h, int32_t c, int32_t v);
 
+/* Cluster-resident path (no reference counterpart): a single network whose
+ * edges, node state and delay ring fit in the shared memory of one
+ * thread-block cluster (<= 16 CTAs of <= 1024 rows) is stepped by
+ * lev_step_n / lev_step_n_async with one launch per block of steps, delayed
+ * phases of other CTAs' nodes read through distributed shared memory, one
+ * cluster barrier per step.  Results are bitwise those of the per-step
+ * kernel.  Eligibility is decided at creation; lev_set_cluster_mode(h, 0)
+ * forces the per-step kernel. */
+int lev_cluster_info(const LevEngine *h, int32_t *eligible, int32_t *enabled,
+                     int32_t *ctas, int32_t *rows_per_cta, int64_t *smem_bytes);
+int lev_set_cluster_mode(LevEngine *h, int32_t enabled);
+
 /* Times every variant on every non-empty class of this engine
  * (trial_steps steps each, after two warm-up steps), keeps the fastest per
  * class, remembers it for later engines of the process with a similar class,

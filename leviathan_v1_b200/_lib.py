@@ -99,6 +99,9 @@ PROTOTYPES = {
     "lev_get_params": (C.c_int, [_P, _i32, C.POINTER(LevParams)]),
     "lev_set_math_mode": (C.c_int, [_P, _i32]),
     "lev_get_vram_usage": (C.c_int, [_P, C.POINTER(C.c_size_t)]),
+    "lev_cluster_info": (C.c_int, [_P, C.POINTER(_i32), C.POINTER(_i32),
+                                   C.POINTER(_i32), C.POINTER(_i32), C.POINTER(_i64)]),
+    "lev_set_cluster_mode": (C.c_int, [_P, _i32]),
     "lev_num_variants": (C.c_int, []),
     "lev_variant_info": (C.c_int, [_i32, C.POINTER(_i32), C.POINTER(_i32),
                                    C.POINTER(_i32)]),

@@ -1,0 +1,309 @@
+// lev_cluster.cuh -- cluster-resident engine for small networks.  Included
+// once, from lev_engine.cu.
+//
+// A network of up to 16 x 1024 nodes whose edges, node state and delay ring
+// fit in the shared memory of one thread-block cluster (up to 16 CTAs, one per
+// SM, 227 KB each) is stepped n times in ONE launch:
+//   * CTA r of the cluster owns rows [r*R, r*R + R), R a multiple of 256, one
+//     thread per row; its SELL-32 slices (col|delay, weights), its node state
+//     and its rows of every ring slot live in its shared memory;
+//   * a delayed phase of a node owned by another CTA is read from that CTA's
+//     shared memory (distributed shared memory, cluster.map_shared_rank);
+//   * one cluster barrier per step orders every ring write before the next
+//     step's reads (with max_delay+2 ring slots, reads and the write of one
+//     step never touch the same slot);
+//   * each 256-node block's (sum cos, sum sin) goes to a double-buffered
+//     array in CTA 0; after the barrier every CTA reduces them in the
+//     reference's order (leviathan_kernel.cu:242-263), so all CTAs compute
+//     the same r and gain without a second barrier.
+// Arithmetic and summation order are those of step_kernel: results are
+// bitwise the same as stepping with step_kernel.
+
+#include <cooperative_groups.h>
+
+namespace lev {
+
+constexpr int kClusterMax = 16;     // CTAs per cluster (non-portable size)
+constexpr int kClusterRowsMax = 1024;
+constexpr int kClusterBlocksMax = kClusterMax * kClusterRowsMax / kTile;  // 64
+
+struct ClusterArgs {
+  const NetDesc *net;
+  NetState *st;
+  const int *row_ptr;
+  const long long *sl_off;
+  const int *sl_len;
+  const uint32_t *sl_cd;
+  float *sl_w;
+  float *theta;
+  float *theta_hat;
+  const float *omega;
+  float *omega_hat;
+  float *ring;
+  float *r_hist;  // [n] (row rpos + k), or null
+  int r_cap;
+  int n_steps;
+  int R;          // rows per CTA (multiple of 256)
+  int edge_cap;   // SELL entries per CTA the shared memory was sized for
+  float dt;
+};
+
+// shared memory layout (bytes, from the dynamic base):
+//   part   float2 [2][kClusterBlocksMax]       block partials (used in CTA 0)
+//   sloff  int    [R/32]   slice start (relative to the CTA's first entry)
+//   sllen  int    [R/32]
+//   th, thh, om, omh  float [R]
+//   ring   float  [bsi][R]
+//   cd     uint32 [edge_cap]
+//   w      float  [edge_cap]
+template <int MATH>
+__global__ void __launch_bounds__(kClusterRowsMax, 1) cluster_kernel(const ClusterArgs a) {
+  namespace cg = cooperative_groups;
+  cg::cluster_group cluster = cg::this_cluster();
+  extern __shared__ __align__(16) unsigned char smem[];
+  __shared__ float s_rc[32];
+  __shared__ float s_rs[32];
+
+  const NetDesc nd = *a.net;
+  const int rank = (int)cluster.block_rank();
+  const int R = a.R;
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const int N = nd.N, bsi = nd.bsi, Np = nd.Np;
+  const int row0 = rank * R;
+  const int row = row0 + tid;
+  const bool live = (tid < R) && (row < N);
+  const int nslices = R / 32;
+
+  float2 *part = reinterpret_cast<float2 *>(smem);
+  int *sloff = reinterpret_cast<int *>(part + 2 * kClusterBlocksMax);
+  int *sllen = sloff + nslices;
+  float *s_th = reinterpret_cast<float *>(sllen + nslices);
+  float *s_thh = s_th + R;
+  float *s_om = s_thh + R;
+  float *s_omh = s_om + R;
+  float *s_ring = s_omh + R;
+  uint32_t *s_cd = reinterpret_cast<uint32_t *>(s_ring + (size_t)bsi * R);
+  float *s_w = reinterpret_cast<float *>(s_cd + a.edge_cap);
+
+  // ---- load this CTA's part of the network --------------------------------
+  const long long sl0 = nd.slice_base + row0 / 32;
+  const int my_slices = max(0, min(nslices, (N - row0 + 31) / 32));
+  const long long ebase = my_slices ? a.sl_off[sl0] : 0;
+  long long eend = ebase;
+  for (int s = tid; s < nslices; s += blockDim.x) {
+    if (s < my_slices) {
+      sloff[s] = (int)(a.sl_off[sl0 + s] - ebase);
+      sllen[s] = a.sl_len[sl0 + s];
+    } else {
+      sloff[s] = 0;
+      sllen[s] = 0;
+    }
+  }
+  if (my_slices) eend = a.sl_off[sl0 + my_slices - 1] + 32LL * a.sl_len[sl0 + my_slices - 1];
+  const int nent = (int)(eend - ebase);
+  for (int k = tid; k < nent; k += blockDim.x) {
+    s_cd[k] = a.sl_cd[ebase + k];
+    s_w[k] = a.sl_w[ebase + k];
+  }
+  int deg = 0;
+  if (live) {
+    const long long gi = nd.node_off + row;
+    s_th[tid] = a.theta[gi];
+    s_thh[tid] = a.theta_hat[gi];
+    s_om[tid] = a.omega[gi];
+    s_omh[tid] = a.omega_hat[gi];
+    const int *rp = a.row_ptr + nd.rp_off + row;
+    deg = rp[1] - rp[0];
+  }
+  for (int s = 0; s < bsi; ++s)
+    if (live) s_ring[(size_t)s * R + tid] = a.ring[nd.ring_off + (long long)s * Np + row];
+  NetState ns = *a.st;
+  int cur = ns.cur, rbuf = ns.rbuf;
+  float g = ns.g, r = ns.r;
+  const int nblocks = (N + kTile - 1) / kTile;
+  const float dt = a.dt;
+  const float eta = nd.eta, gamma = nd.gamma, lam = nd.lam;
+  const float w_min = nd.w_min, w_max = nd.w_max;
+  const unsigned mask = 0xffffffffu;
+  cluster.sync();
+
+  float2 *part0 = cluster.map_shared_rank(part, 0);
+  __shared__ float s_g;
+  for (int step = 0; step < a.n_steps; ++step) {
+    // ---- r and gain of the previous step: warp 0 of every CTA reduces the
+    // block partials (same order everywhere) and shares g with its CTA ----
+    if (step > 0) {
+      if (warp == 0) {
+        const float2 *pb = part0 + ((step - 1) & 1) * kClusterBlocksMax;
+        float sum_cos = 0.0f, sum_sin = 0.0f;
+        for (int k = lane; k < nblocks; k += 32) {
+          const float2 v = pb[k];
+          sum_cos += v.x;
+          sum_sin += v.y;
+        }
+#pragma unroll
+        for (int off = 16; off > 0; off /= 2) {
+          sum_cos += __shfl_down_sync(mask, sum_cos, off);
+          sum_sin += __shfl_down_sync(mask, sum_sin, off);
+        }
+        if (lane == 0) {
+          float inv_N = 1.0f / (float)N;
+          r = sqrtf(sum_cos * sum_cos + sum_sin * sum_sin) * inv_N;
+          if (nd.ctrl) g = gain_controller(g, r, dt, nd);
+          s_g = g;
+          if (rank == 0 && a.r_hist) {
+            const int k = ns.rpos + step - 1;
+            if (k < a.r_cap) a.r_hist[k] = r;
+          }
+        }
+      }
+      __syncthreads();
+      g = s_g;
+    }
+    // ---- predictor --------------------------------------------------------
+    float th = 0.0f, eps = 0.0f;
+    if (live) {
+      th = s_th[tid];
+      const float thh = s_thh[tid];
+      const float wh = s_omh[tid];
+      float diff = th - thh;
+      diff = wrap_pm_pi(diff);
+      eps = sinf(diff);
+      s_thh[tid] = thh + dt * wh;
+      s_omh[tid] = wh + nd.kappa_w * dt * eps;
+    }
+    const float my_eps = fabsf(eps);
+    // ---- edges --------------------------------------------------------------
+    float local_sum = 0.0f;
+    if (warp < my_slices) {
+      const int len = sllen[warp];
+      const int base = sloff[warp] + lane;
+      constexpr int U = 8;
+      for (int k0 = 0; k0 < len; k0 += U) {
+        uint32_t p[U];
+        float wv[U], dj[U];
+#pragma unroll
+        for (int u = 0; u < U; ++u) {
+          const bool in = k0 + u < deg;
+          p[u] = in ? s_cd[base + 32 * (k0 + u)] : 0u;
+          wv[u] = in ? s_w[base + 32 * (k0 + u)] : 0.0f;
+        }
+#pragma unroll
+        for (int u = 0; u < U; ++u) {
+          int slot = cur - (int)(p[u] & 255u);
+          slot += (slot < 0) ? bsi : 0;
+          const int j = (int)(p[u] >> 8);
+          const int owner = j / R;
+          const int loc = j - owner * R;
+          const float *src = (owner == rank) ? s_ring : cluster.map_shared_rank(s_ring, owner);
+          dj[u] = src[(size_t)slot * R + loc];
+        }
+#pragma unroll
+        for (int u = 0; u < U; ++u) {
+          if (k0 + u < deg) {
+            const float delayed_j = dj[u];
+            float diff = delayed_j - th;
+            diff = wrap_pm_pi(diff);
+            float w = wv[u];
+            float sin_diff, cos_diff;
+            lev_sincos<MATH>(diff, &sin_diff, &cos_diff);
+            local_sum += w * sin_diff;
+            float dw = dt * (eta * cos_diff * (1.0f - gamma * my_eps) - lam * w);
+            w += dw;
+            if (!isfinite(w)) w = w_min;
+            w = fmaxf(w_min, fminf(w_max, w));
+            s_w[base + 32 * (k0 + u)] = w;
+          }
+        }
+      }
+    }
+    // ---- integrate ----------------------------------------------------------
+    int nxt = cur + 1;
+    if (nxt == bsi) nxt = 0;
+    float my_cos = 0.0f, my_sin = 0.0f;
+    if (live) {
+      float inc = dt * (s_om[tid] + g * local_sum - nd.alpha * eps);
+      float x = th + inc;
+      x = wrap_0_2pi(x);
+      if (!isfinite(x)) x = 0.0f;
+      s_th[tid] = x;
+      s_ring[(size_t)nxt * R + tid] = x;
+      lev_sincos<MATH>(x, &my_sin, &my_cos);
+    }
+    // ---- 256-node block partials (leviathan_kernel.cu:198-233) --------------
+#pragma unroll
+    for (int off = 16; off > 0; off /= 2) {
+      my_cos += __shfl_down_sync(mask, my_cos, off);
+      my_sin += __shfl_down_sync(mask, my_sin, off);
+    }
+    if (lane == 0) {
+      s_rc[warp] = my_cos;
+      s_rs[warp] = my_sin;
+    }
+    __syncthreads();
+    if ((warp & 7) == 0 && warp * 32 < R) {  // first warp of each 256-row block
+      const int b = warp >> 3;                // block within this CTA
+      float c = (lane < 8) ? s_rc[warp + lane] : 0.0f;
+      float s = (lane < 8) ? s_rs[warp + lane] : 0.0f;
+#pragma unroll
+      for (int off = 16; off > 0; off /= 2) {
+        c += __shfl_down_sync(mask, c, off);
+        s += __shfl_down_sync(mask, s, off);
+      }
+      const int gb = row0 / kTile + b;
+      if (lane == 0 && gb < nblocks)
+        part0[(step & 1) * kClusterBlocksMax + gb] = make_float2(c, s);
+    }
+    cur = nxt;
+    rbuf = (rbuf + 1 == nd.max_delay + 1) ? 0 : rbuf + 1;
+    cluster.sync();
+  }
+  // ---- r of the last step, then write the state back ------------------------
+  if (a.n_steps > 0) {
+    const float2 *pb = part0 + ((a.n_steps - 1) & 1) * kClusterBlocksMax;
+    float sum_cos = 0.0f, sum_sin = 0.0f;
+    for (int k = lane; k < nblocks; k += 32) {
+      const float2 v = pb[k];
+      sum_cos += v.x;
+      sum_sin += v.y;
+    }
+#pragma unroll
+    for (int off = 16; off > 0; off /= 2) {
+      sum_cos += __shfl_down_sync(mask, sum_cos, off);
+      sum_sin += __shfl_down_sync(mask, sum_sin, off);
+    }
+    sum_cos = __shfl_sync(mask, sum_cos, 0);
+    sum_sin = __shfl_sync(mask, sum_sin, 0);
+    float inv_N = 1.0f / (float)N;
+    r = sqrtf(sum_cos * sum_cos + sum_sin * sum_sin) * inv_N;
+    if (nd.ctrl) g = gain_controller(g, r, dt, nd);
+    if (rank == 0 && tid == 0) {
+      if (a.r_hist) {
+        const int k = ns.rpos + a.n_steps - 1;
+        if (k < a.r_cap) a.r_hist[k] = r;
+      }
+      NetState o = ns;
+      o.g = g;
+      o.r = r;
+      o.cur = cur;
+      o.rbuf = rbuf;
+      o.t = ns.t + a.n_steps;
+      o.rpos = ns.rpos + a.n_steps;
+      o.ticket = 0u;
+      *a.st = o;
+    }
+  }
+  if (live) {
+    const long long gi = nd.node_off + row;
+    a.theta[gi] = s_th[tid];
+    a.theta_hat[gi] = s_thh[tid];
+    a.omega_hat[gi] = s_omh[tid];
+    for (int s = 0; s < bsi; ++s)
+      a.ring[nd.ring_off + (long long)s * Np + row] = s_ring[(size_t)s * R + tid];
+  }
+  for (int k = tid; k < nent; k += blockDim.x) a.sl_w[ebase + k] = s_w[k];
+  // no CTA may leave while a peer can still read its shared memory
+  cluster.sync();
+}
+
+}  // namespace lev

@@ -20,6 +20,7 @@
 
 #include "leviathan_b200.h"
 #include "lev_kernels.cuh"
+#include "lev_cluster.cuh"
 
 namespace lev {
 
@@ -151,6 +152,12 @@ struct LevEngine {
   std::map<std::tuple<int, uint32_t, int>, GraphEntry> graphs;
 
   TileClass classes[kNumClasses];
+
+  // cluster-resident path for small single networks (lev_cluster.cuh)
+  bool cluster_ok = false;   // eligible and launchable on this device
+  bool use_cluster = true;   // may step blocks use it
+  int cluster_R = 0, cluster_C = 0, cluster_edge_cap = 0;
+  size_t cluster_smem = 0;
 };
 
 struct LeviathanHandle {
@@ -368,16 +375,128 @@ int get_graph(LevEngine *h, int len, float dt, cudaGraphExec_t *out) {
   return LEV_OK;
 }
 
-// Enqueue n steps as graph replays; if stage != null, the r history of every
-// block is copied into stage[n][num_nets] (pinned host memory).
+// One launch of the cluster-resident kernel: `len` steps, r history rows
+// 0..len-1 in d_rhist.
+int launch_cluster(LevEngine *h, float dt, int len) {
+  reset_rpos_kernel<<<1, 128, 0, h->stream>>>(h->d_st, h->num_nets);
+  ClusterArgs ca;
+  ca.net = h->d_nets;
+  ca.st = h->d_st;
+  ca.row_ptr = h->d_row_ptr;
+  ca.sl_off = h->d_sl_off;
+  ca.sl_len = h->d_sl_len;
+  ca.sl_cd = h->d_sl_cd;
+  ca.sl_w = h->d_sl_w;
+  ca.theta = h->d_theta;
+  ca.theta_hat = h->d_theta_hat;
+  ca.omega = h->d_omega;
+  ca.omega_hat = h->d_omega_hat;
+  ca.ring = h->d_ring;
+  ca.r_hist = h->d_rhist;
+  ca.r_cap = h->block_len;
+  ca.n_steps = len;
+  ca.R = h->cluster_R;
+  ca.edge_cap = h->cluster_edge_cap;
+  ca.dt = dt;
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3(h->cluster_C);
+  cfg.blockDim = dim3(h->cluster_R);
+  cfg.dynamicSmemBytes = h->cluster_smem;
+  cfg.stream = h->stream;
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeClusterDimension;
+  attr[0].val.clusterDim.x = h->cluster_C;
+  attr[0].val.clusterDim.y = 1;
+  attr[0].val.clusterDim.z = 1;
+  cfg.attrs = attr;
+  cfg.numAttrs = 1;
+  if (h->math_mode == LEV_MATH_ACCURATE)
+    LEV_TRY_CUDA(cudaLaunchKernelEx(&cfg, cluster_kernel<1>, ca));
+  else
+    LEV_TRY_CUDA(cudaLaunchKernelEx(&cfg, cluster_kernel<0>, ca));
+  return LEV_OK;
+}
+
+// Small single networks: choose rows per CTA and check that the cluster
+// kernel can run (shared memory, cluster size, occupancy).
+void setup_cluster(LevEngine *h, const std::vector<long long> &sl_off,
+                   const std::vector<int> &sl_len) {
+  h->cluster_ok = false;
+  if (h->num_nets != 1) return;
+  const NetDesc &d = h->h_nets[0];
+  int dev = 0, max_smem = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess) return;
+  if (cudaDeviceGetAttribute(&max_smem, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev) !=
+      cudaSuccess)
+    return;
+  for (int R = kTile; R <= kClusterRowsMax; R += kTile) {
+    const int C = (d.N + R - 1) / R;
+    if (C > kClusterMax) continue;
+    long long cap = 0;
+    for (int c = 0; c < C; ++c) {
+      long long e = 0;
+      for (int s = c * R / 32; s < std::min<long long>((c + 1) * R / 32, (d.N + 31) / 32); ++s)
+        e += 32LL * sl_len[d.slice_base + s];
+      cap = std::max(cap, e);
+    }
+    const size_t smem = sizeof(float2) * 2 * kClusterBlocksMax + sizeof(int) * 2 * (R / 32) +
+                        sizeof(float) * 4 * R + sizeof(float) * (size_t)d.bsi * R +
+                        8 * (size_t)cap;
+    if (smem + 1024 > (size_t)max_smem) continue;
+    bool ok = true;
+    for (int m = 0; m < 2 && ok; ++m) {
+      const void *fn = m ? reinterpret_cast<const void *>(cluster_kernel<1>)
+                         : reinterpret_cast<const void *>(cluster_kernel<0>);
+      ok = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) ==
+               cudaSuccess &&
+           cudaFuncSetAttribute(fn, cudaFuncAttributeNonPortableClusterSizeAllowed, 1) ==
+               cudaSuccess;
+      if (ok) {
+        cudaLaunchConfig_t cfg = {};
+        cfg.gridDim = dim3(C);
+        cfg.blockDim = dim3(R);
+        cfg.dynamicSmemBytes = smem;
+        cudaLaunchAttribute attr[1];
+        attr[0].id = cudaLaunchAttributeClusterDimension;
+        attr[0].val.clusterDim.x = C;
+        attr[0].val.clusterDim.y = 1;
+        attr[0].val.clusterDim.z = 1;
+        cfg.attrs = attr;
+        cfg.numAttrs = 1;
+        int clusters = 0;
+        ok = cudaOccupancyMaxActiveClusters(&clusters, fn, &cfg) == cudaSuccess && clusters >= 1;
+      }
+    }
+    cudaGetLastError();  // clear a refused attribute, if any
+    if (!ok) continue;
+    h->cluster_ok = true;
+    h->cluster_R = R;
+    h->cluster_C = C;
+    h->cluster_edge_cap = (int)cap;
+    h->cluster_smem = smem;
+    // measured on B200: faster than per-step graph replay up to ~8 CTAs of
+    // distributed gathers; lev_autotune times both and decides per engine
+    h->use_cluster = C <= 8;
+    return;
+  }
+}
+
+// Enqueue n steps as graph replays (or cluster-kernel launches for small
+// networks); if stage != null, the r history of every block is copied into
+// stage[n][num_nets] (pinned host memory).
 int enqueue_steps(LevEngine *h, float dt, int n, float *stage) {
   int done = 0;
   while (done < n) {
     const int len = std::min(h->block_len, n - done);
-    cudaGraphExec_t ex;
-    int rc = get_graph(h, len, dt, &ex);
-    if (rc != LEV_OK) return rc;
-    LEV_TRY_CUDA(cudaGraphLaunch(ex, h->stream));
+    if (h->cluster_ok && h->use_cluster) {
+      int rc = launch_cluster(h, dt, len);
+      if (rc != LEV_OK) return rc;
+    } else {
+      cudaGraphExec_t ex;
+      int rc = get_graph(h, len, dt, &ex);
+      if (rc != LEV_OK) return rc;
+      LEV_TRY_CUDA(cudaGraphLaunch(ex, h->stream));
+    }
     if (stage) {
       LEV_TRY_CUDA(cudaMemcpyAsync(
           stage + (size_t)done * h->num_nets, h->d_rhist,
@@ -568,6 +687,7 @@ int create_impl(LevEngine **out, int num_nets, const int32_t *Ns,
                                   cudaGetErrorString(ce));
   }
   int rc = prepare_step_kernels();
+  setup_cluster(h, h_sl_off, h_sl_len);
 #define LEV_ALLOC(ptr, count)                      \
   if (rc == LEV_OK) rc = dev_alloc(h, &(ptr), (count));
   LEV_ALLOC(h->d_nets, (size_t)num_nets);
@@ -1196,6 +1316,23 @@ int lev_set_math_mode(LevEngine *h, int32_t math_mode) {
   return LEV_OK;
 }
 
+int lev_cluster_info(const LevEngine *h, int32_t *eligible, int32_t *enabled,
+                     int32_t *ctas, int32_t *rows_per_cta, int64_t *smem_bytes) {
+  if (!h) return fail(LEV_ERR_ARG, "null handle");
+  if (eligible) *eligible = h->cluster_ok ? 1 : 0;
+  if (enabled) *enabled = h->use_cluster ? 1 : 0;
+  if (ctas) *ctas = h->cluster_C;
+  if (rows_per_cta) *rows_per_cta = h->cluster_R;
+  if (smem_bytes) *smem_bytes = (int64_t)h->cluster_smem;
+  return LEV_OK;
+}
+
+int lev_set_cluster_mode(LevEngine *h, int32_t enabled) {
+  if (!h) return fail(LEV_ERR_ARG, "null handle");
+  h->use_cluster = enabled != 0;
+  return LEV_OK;
+}
+
 int lev_num_variants(void) { return kNumVariants; }
 
 int lev_variant_info(int32_t v, int32_t *unroll, int32_t *pipelined,
@@ -1329,6 +1466,22 @@ int lev_autotune(LevEngine *h, float dt, int32_t trial_steps,
     if (variant_out) variant_out[c] = best_v;
     std::lock_guard<std::mutex> lk(g_tune_mu);
     g_tune_cache[tune_key(tc, c)] = best_v;
+  }
+  // small single networks: cluster-resident kernel or per-step graph replay
+  if (rc == LEV_OK && h->cluster_ok) {
+    const int n = std::max(trial_steps, 32);
+    float t_mode[2] = {0.0f, 0.0f};
+    for (int m = 1; m >= 0 && rc == LEV_OK; --m) {
+      h->use_cluster = (m == 1);
+      rc = enqueue_steps(h, dt, n, nullptr);  // warm-up (graph instantiation)
+      if (rc != LEV_OK) break;
+      cudaEventRecord(e0, h->stream);
+      rc = enqueue_steps(h, dt, n, nullptr);
+      cudaEventRecord(e1, h->stream);
+      if (rc == LEV_OK && cudaEventSynchronize(e1) == cudaSuccess)
+        cudaEventElapsedTime(&t_mode[m], e0, e1);
+    }
+    h->use_cluster = rc == LEV_OK && t_mode[1] <= t_mode[0];
   }
   if (e0) cudaEventDestroy(e0);
   if (e1) cudaEventDestroy(e1);

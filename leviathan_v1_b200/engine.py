@@ -271,6 +271,18 @@ class _EngineBase:
     def set_variant(self, cls: int, variant: int) -> None:
         check(self._lib.lev_set_variant(self.handle, int(cls), int(variant)))
 
+    # -- cluster-resident path (small single networks) ---------------------
+    def cluster_info(self) -> dict:
+        el, en, c, r = C.c_int32(), C.c_int32(), C.c_int32(), C.c_int32()
+        sm = C.c_int64()
+        check(self._lib.lev_cluster_info(self.handle, C.byref(el), C.byref(en), C.byref(c),
+                                         C.byref(r), C.byref(sm)))
+        return dict(eligible=bool(el.value), enabled=bool(en.value), ctas=c.value,
+                    rows_per_cta=r.value, smem_bytes=sm.value)
+
+    def set_cluster_mode(self, enabled: bool) -> None:
+        check(self._lib.lev_set_cluster_mode(self.handle, 1 if enabled else 0))
+
     # -- checkpoint ---------------------------------------------------------
     def get_state(self) -> dict:
         """Full engine state (the reference exposes no such getter)."""

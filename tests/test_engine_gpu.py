@@ -198,6 +198,45 @@ def test_batch_equals_individual_engines():
     be.close()
 
 
+@pytest.mark.parametrize("N,k,md,ctrl", [(1000, 20, 50, 1), (700, 8, 10, 0),
+                                         (4096, 32, 64, 1), (3000, 12, 0, 1),
+                                         (16000, 8, 8, 1)])
+def test_cluster_path_bit_identical(N, k, md, ctrl):
+    """The cluster-resident kernel (whole network in the shared memory of one
+    thread-block cluster, many steps per launch) gives bitwise the results of
+    the per-step kernel."""
+    net = make_network(N, k, 0.1, md, seed=N + md, delay_lo=min(1, md))
+    a = LeviathanEngine(*net.engine_args(), params=dict(gain_controller=ctrl))
+    b = LeviathanEngine(*net.engine_args(), params=dict(gain_controller=ctrl))
+    info = a.cluster_info()
+    assert info["eligible"], info
+    b.set_cluster_mode(False)
+    ra = np.concatenate([a.step_n(DT, 5), a.step_n(DT, 300)])
+    rb = np.concatenate([b.step_n(DT, 5), b.step_n(DT, 300)])
+    np.testing.assert_array_equal(ra, rb)
+    np.testing.assert_array_equal(a.get_theta(), b.get_theta())
+    np.testing.assert_array_equal(a.get_weights(), b.get_weights())
+    ga, gb = a.get_predictor(), b.get_predictor()
+    np.testing.assert_array_equal(ga[0], gb[0])
+    np.testing.assert_array_equal(ga[1], gb[1])
+    assert a.get_gain() == b.get_gain() and a.step_count() == b.step_count() == 305
+    ring_a, bi_a = a.get_ring()
+    ring_b, bi_b = b.get_ring()
+    assert bi_a == bi_b
+    np.testing.assert_array_equal(ring_a, ring_b)
+    # and a single step after the block still continues identically
+    assert a.step(DT) == b.step(DT)
+    a.close()
+    b.close()
+
+
+def test_cluster_path_not_used_when_too_large():
+    net = make_network(40_000, 16, 0.1, 20, seed=1)
+    e = LeviathanEngine(*net.engine_args())
+    assert not e.cluster_info()["eligible"]
+    e.close()
+
+
 def test_autotune_leaves_simulation_unchanged():
     nets = [make_network(n, k, 0.1, 20, seed=s)
             for n, k, s in [(3000, 8, 1), (2000, 20, 2), (5000, 32, 3)]]
