@@ -363,6 +363,25 @@ int lev_step_noalloc(int32_t N, int32_t max_delay, int64_t t,
                      void *stream);
 
 /* ------------------------------------------------------------------------ */
+/* Topology and initial state on the device                                  */
+/* ------------------------------------------------------------------------ */
+
+/* Seeded Watts-Strogatz graph built on the current device (replaces the
+ * host networkx/scipy construction of python/leviathan_h100.py:34-55): ring
+ * lattice of k/2 neighbours per side, every lattice edge rewired with
+ * probability p to a uniform target avoiding self-loops and multi-edges;
+ * canonical symmetric CSR (columns sorted), E = N*k.  Initial state drawn
+ * per position: delays uniform in [delay_lo, delay_hi], weights uniform in
+ * [w_lo, w_hi), theta uniform in [0, 2pi), omega ~ Normal(mean, std).
+ * Deterministic for a seed.  Outputs are HOST arrays: row_ptr[N+1],
+ * col_idx[E], delays[E], weights[E], theta[N], omega[N]. */
+int lev_gen_ws(int32_t N, int32_t k, double p, uint64_t seed,
+               int32_t delay_lo, int32_t delay_hi, float w_lo, float w_hi,
+               float omega_mean, float omega_std, int32_t *row_ptr,
+               int32_t *col_idx, uint8_t *delays, float *weights,
+               float *theta, float *omega);
+
+/* ------------------------------------------------------------------------ */
 /* Reference C ABI (leviathan_kernel.cu:21-499), same symbols and signatures */
 /* ------------------------------------------------------------------------ */
 typedef struct LeviathanHandle LeviathanHandle;

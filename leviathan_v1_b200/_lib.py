@@ -121,6 +121,8 @@ PROTOTYPES = {
     "lev_step_noalloc":(C.c_int, [_i32, _i32, _i64, _P, _P, _P, _P, _P, _P, _P,
                                    _P, _P, _P, _P, C.POINTER(LevParams), _f32,
                                    _i32, _P]),
+    "lev_gen_ws": (C.c_int, [_i32, _i32, C.c_double, C.c_uint64, _i32, _i32, _f32,
+                             _f32, _f32, _f32, _P, _P, _P, _P, _P, _P]),
     # reference ABI (leviathan_kernel.cu:21-499)
     "leviathan_init": (_P, [C.c_int, C.c_int, _P, _P, _P, _P, _P, _P, _P]),
     "leviathan_step": (_f32, [_P, _f32]),

@@ -1591,6 +1591,125 @@ LevEngine *leviathan_engine(LeviathanHandle *handle) {
 // lev_adjoint.cuh.
 // ===========================================================================
 #include "lev_adjoint.cuh"
+#include "lev_graphgen.cuh"
+
+namespace lev {
+__global__ void ws_table_init_kernel(WsSlot *t, unsigned long long n) {
+  for (unsigned long long k = blockIdx.x * (unsigned long long)blockDim.x + threadIdx.x;
+       k < n; k += (unsigned long long)gridDim.x * blockDim.x) {
+    t[k].key = 0ull;
+    t[k].owner = 0xFFFFFFFFu;
+    t[k].accepted = 0u;
+  }
+}
+}  // namespace lev
+
+extern "C" int lev_gen_ws(int32_t N, int32_t k, double p, uint64_t seed,
+                          int32_t delay_lo, int32_t delay_hi, float w_lo,
+                          float w_hi, float omega_mean, float omega_std,
+                          int32_t *row_ptr, int32_t *col_idx, uint8_t *delays,
+                          float *weights, float *theta, float *omega) {
+  if (N < 3 || N >= (1 << 24)) return fail(LEV_ERR_ARG, "N must be in [3, 2^24)");
+  if (k < 2 || (k & 1) || k >= N) return fail(LEV_ERR_ARG, "k must be even, 2 <= k < N");
+  if (!(p >= 0.0 && p <= 1.0)) return fail(LEV_ERR_ARG, "p must be in [0, 1]");
+  if (delay_lo < 0 || delay_hi > 255 || delay_lo > delay_hi)
+    return fail(LEV_ERR_ARG, "delays must satisfy 0 <= lo <= hi <= 255");
+  if (!row_ptr || !col_idx || !delays || !weights || !theta || !omega)
+    return fail(LEV_ERR_ARG, "null output array");
+  const long long half = k / 2, n_lat = (long long)N * half, E = 2 * n_lat;
+  if (E >= (1LL << 31)) return fail(LEV_ERR_ARG, "N*k must be below 2^31");
+  cudaStream_t s;
+  LEV_TRY_CUDA(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking));
+  // table: >= 4x the expected number of rewired edges (load factor <= 1/4)
+  unsigned long long tsize = 1024;
+  while (tsize < (unsigned long long)(4.0 * p * n_lat + 1024)) tsize <<= 1;
+  int *target = nullptr, *deg = nullptr, *rp = nullptr, *cursor = nullptr, *col = nullptr;
+  unsigned int *pend[2] = {nullptr, nullptr}, *cnt = nullptr;
+  long long *cand = nullptr;
+  WsSlot *table = nullptr;
+  uint8_t *dl = nullptr;
+  float *w = nullptr, *th = nullptr, *om = nullptr;
+  std::vector<void *> bufs;
+  auto cleanup = [&]() {
+    for (void *b : bufs) cudaFree(b);
+    cudaStreamDestroy(s);
+  };
+  auto alloc = [&](void **ptr, size_t bytes) {
+    cudaError_t e = cudaMalloc(ptr, std::max<size_t>(bytes, 4));
+    if (e == cudaSuccess) bufs.push_back(*ptr);
+    return e == cudaSuccess;
+  };
+  bool ok = alloc((void **)&target, sizeof(int) * n_lat) &&
+            alloc((void **)&deg, sizeof(int) * N) &&
+            alloc((void **)&rp, sizeof(int) * (N + 1)) &&
+            alloc((void **)&cursor, sizeof(int) * N) &&
+            alloc((void **)&col, sizeof(int) * E) &&
+            alloc((void **)&pend[0], sizeof(unsigned) * n_lat) &&
+            alloc((void **)&pend[1], sizeof(unsigned) * n_lat) &&
+            alloc((void **)&cnt, sizeof(unsigned) * 2) &&
+            alloc((void **)&cand, sizeof(long long) * n_lat) &&
+            alloc((void **)&table, sizeof(WsSlot) * tsize) &&
+            alloc((void **)&dl, E) && alloc((void **)&w, sizeof(float) * E) &&
+            alloc((void **)&th, sizeof(float) * N) && alloc((void **)&om, sizeof(float) * N);
+  if (!ok) {
+    cleanup();
+    return fail(LEV_ERR_NOMEM, "lev_gen_ws: device allocation failed");
+  }
+  WsArgs a;
+  a.N = N;
+  a.half = (int)half;
+  a.p = p;
+  a.seed = seed;
+  const int G = 148 * 8, B = 256;
+  cudaMemsetAsync(cnt, 0, sizeof(unsigned) * 2, s);
+  cudaMemsetAsync(deg, 0, sizeof(int) * N, s);
+  cudaMemsetAsync(cursor, 0, sizeof(int) * N, s);
+  ws_table_init_kernel<<<G, B, 0, s>>>(table, tsize);
+  ws_init_kernel<<<G, B, 0, s>>>(a, n_lat, target, pend[0], cnt);
+  unsigned int n_pend = 0;
+  cudaMemcpyAsync(&n_pend, cnt, sizeof(unsigned), cudaMemcpyDeviceToHost, s);
+  cudaError_t ce = cudaStreamSynchronize(s);
+  int cur = 0, round = 0;
+  while (ce == cudaSuccess && n_pend > 0) {
+    if (++round > 200) {
+      cleanup();
+      return fail(LEV_ERR_ARG, "lev_gen_ws: rewiring did not settle (graph too dense)");
+    }
+    cudaMemsetAsync(cnt + 1, 0, sizeof(unsigned), s);
+    ws_propose_kernel<<<G, B, 0, s>>>(a, round, pend[cur], n_pend, table, tsize - 1, cand);
+    ws_resolve_kernel<<<G, B, 0, s>>>(a, round, pend[cur], n_pend, table, cand, target,
+                                      pend[cur ^ 1], cnt + 1);
+    cudaMemcpyAsync(&n_pend, cnt + 1, sizeof(unsigned), cudaMemcpyDeviceToHost, s);
+    ce = cudaStreamSynchronize(s);
+    cur ^= 1;
+  }
+  if (ce == cudaSuccess) {
+    ws_degree_kernel<<<G, B, 0, s>>>(a, n_lat, target, deg);
+    ws_scan_kernel<<<1, 1024, 0, s>>>(deg, rp, N);
+    ws_fill_kernel<<<G, B, 0, s>>>(a, n_lat, target, rp, cursor, col);
+    WsStateArgs st;
+    st.seed = seed ^ 0x5A17E5EEDull;
+    st.delay_lo = delay_lo;
+    st.delay_hi = delay_hi;
+    st.w_lo = w_lo;
+    st.w_hi = w_hi;
+    st.omega_mean = omega_mean;
+    st.omega_std = omega_std;
+    ws_finish_kernel<<<G, B, 0, s>>>(st, N, rp, col, dl, w, th, om);
+    ce = cudaGetLastError();
+  }
+  if (ce == cudaSuccess) ce = cudaMemcpyAsync(row_ptr, rp, sizeof(int) * (N + 1), cudaMemcpyDeviceToHost, s);
+  if (ce == cudaSuccess) ce = cudaMemcpyAsync(col_idx, col, sizeof(int) * E, cudaMemcpyDeviceToHost, s);
+  if (ce == cudaSuccess) ce = cudaMemcpyAsync(delays, dl, E, cudaMemcpyDeviceToHost, s);
+  if (ce == cudaSuccess) ce = cudaMemcpyAsync(weights, w, sizeof(float) * E, cudaMemcpyDeviceToHost, s);
+  if (ce == cudaSuccess) ce = cudaMemcpyAsync(theta, th, sizeof(float) * N, cudaMemcpyDeviceToHost, s);
+  if (ce == cudaSuccess) ce = cudaMemcpyAsync(omega, om, sizeof(float) * N, cudaMemcpyDeviceToHost, s);
+  if (ce == cudaSuccess) ce = cudaStreamSynchronize(s);
+  cleanup();
+  if (ce != cudaSuccess)
+    return fail(LEV_ERR_CUDA, std::string("lev_gen_ws: ") + cudaGetErrorString(ce));
+  return LEV_OK;
+}
 
 namespace lev {
 

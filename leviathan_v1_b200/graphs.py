@@ -165,6 +165,36 @@ def make_network(N: int, k: int, p: float, max_delay: int, seed: int, *,
                    meta=dict(k=k, p=p, seed=seed, generator=generator))
 
 
+def make_network_gpu(N: int, k: int, p: float, max_delay: int, seed: int, *,
+                     delay_lo: int = 1, delay_hi: int | None = None,
+                     omega_mean: float = 0.0, omega_std: float = 1.0,
+                     w_lo: float = 0.0, w_hi: float = 1.0) -> Network:
+    """Seeded Watts-Strogatz network and initial state built on the GPU
+    (``lev_gen_ws``): the same random-graph model as ``ws_csr`` with device
+    random streams, in milliseconds at N = 10^6."""
+    import ctypes as C
+
+    from . import _lib
+
+    lib = _lib.load()
+    if delay_hi is None:
+        delay_hi = max_delay
+    E = N * k
+    rp = np.empty(N + 1, np.int32)
+    col = np.empty(E, np.int32)
+    dl = np.empty(E, np.uint8)
+    w = np.empty(E, np.float32)
+    th = np.empty(N, np.float32)
+    om = np.empty(N, np.float32)
+    P = lambda a: C.c_void_p(a.ctypes.data)
+    _lib.check(lib.lev_gen_ws(int(N), int(k), float(p), int(seed) & (2**64 - 1),
+                              int(delay_lo), int(delay_hi), float(w_lo), float(w_hi),
+                              float(omega_mean), float(omega_std), P(rp), P(col), P(dl),
+                              P(w), P(th), P(om)))
+    return Network(N, max_delay, rp, col, dl, w, th, th.copy(), om,
+                   meta=dict(k=k, p=p, seed=seed, generator="gpu"))
+
+
 # ---------------------------------------------------------------------------
 # Benchmark configurations (synthetic, seeded)
 # ---------------------------------------------------------------------------

@@ -302,6 +302,41 @@ def test_invariants_at_scale():
     e.close()
 
 
+@pytest.mark.parametrize("N,k,p", [(5000, 10, 0.1), (100_000, 32, 0.1), (2000, 8, 0.0),
+                                   (300, 20, 1.0)])
+def test_gpu_graph_generator(N, k, p):
+    from leviathan_v1_b200.graphs import make_network_gpu
+
+    a = make_network_gpu(N, k, p, 50, seed=7)
+    b = make_network_gpu(N, k, p, 50, seed=7)
+    c = make_network_gpu(N, k, p, 50, seed=8)
+    rp, col = a.row_ptr, a.col_idx
+    assert rp[0] == 0 and rp[-1] == N * k and np.all(np.diff(rp) >= 0)
+    rows = np.repeat(np.arange(N), np.diff(rp))
+    assert np.all((col >= 0) & (col < N)) and not np.any(rows == col)
+    key = rows.astype(np.int64) * N + col
+    assert np.all(np.diff(key) > 0)  # sorted, no multi-edges
+    assert np.array_equal(np.sort(key), np.sort(col.astype(np.int64) * N + rows))  # symmetric
+    for x, y in zip(a.engine_args()[2:], b.engine_args()[2:]):
+        np.testing.assert_array_equal(x, y)  # deterministic
+    if p > 0:
+        assert not np.array_equal(a.col_idx, c.col_idx)
+        d = np.abs(rows - col)
+        far = np.mean(np.minimum(d, N - d) > k // 2)
+        assert abs(far - p) < 0.02 + 0.1 * p * (N < 1000)
+    else:
+        d = np.abs(rows - col)
+        assert np.all(np.minimum(d, N - d) <= k // 2)
+    assert a.delays.min() >= 1 and a.delays.max() <= 50
+    assert np.all((a.weights >= 0) & (a.weights < 1))
+    assert np.all((a.theta >= 0) & (a.theta <= np.float32(2 * np.pi)))
+    if N >= 5000:
+        assert abs(float(a.omega.mean())) < 0.1 and abs(float(a.omega.std()) - 1) < 0.1
+    e = LeviathanEngine(*a.engine_args())
+    assert np.all(np.isfinite(e.step_n(DT, 20)))
+    e.close()
+
+
 def test_invalid_topology_rejected_on_device():
     net = make_network(500, 8, 0.1, 10, seed=1)
     col = net.col_idx.copy()
