@@ -433,6 +433,8 @@ def run_ours(args, rank, world, local):
     # the in-project autotuner picks the step-kernel variant for this degree
     # distribution (state is restored; later engines of the process reuse it)
     tune = eng.autotune(DT, trial_steps=10)
+    pair_info = [c for c in eng.pair_info() if c["cls"] == max(tune["chosen"]) or True]
+    pair_info = [c for c, t in zip(eng.pair_info(), eng.tuning()) if t["tiles"]]
     stream = torch.cuda.ExternalStream(eng.stream_ptr)
     sampler = ClockSampler(torch.cuda.current_device()).start()
 
@@ -496,7 +498,8 @@ def run_ours(args, rank, world, local):
                      "unit": "GB/s", "frac": achieved / peak, "peak_kind": peak_kind,
                      "traffic": traffic, "kernel": "lev::step_kernel<0,...>",
                      "algorithmic_bytes_per_launch": alg,
-                     "variant": tune["variants"][max(tune["chosen"])] if tune else None},
+                     "variant": tune["variants"][max(tune["chosen"])] if tune else None,
+                     "two_steps_per_launch": pair_info[0]},
         "e2e": e2e,
         "gpu_launches": K + (K + 255) // 256,
         "clocks": clocks,

@@ -21,7 +21,7 @@ LIB_NAME = "libleviathan_b200.so"
 LIB_PATH = os.path.join(LIB_DIR, LIB_NAME)
 
 SOURCES = ["lev_engine.cu"]
-HEADERS = ["lev_kernels.cuh"]
+HEADERS = sorted(f for f in os.listdir(CSRC) if f.endswith(".cuh"))
 
 ARCH_FLAGS = ["-gencode", "arch=compute_100a,code=sm_100a"]
 NVCC_FLAGS = [

@@ -20,6 +20,7 @@
 
 #include "leviathan_b200.h"
 #include "lev_kernels.cuh"
+#include "lev_pair.cuh"
 #include "lev_cluster.cuh"
 
 namespace lev {
@@ -75,6 +76,20 @@ static const StepVariant kVariants[] = {
 #undef LEV_VARIANT
 constexpr int kNumVariants = sizeof(kVariants) / sizeof(kVariants[0]);
 
+// Two-steps-per-launch variants (lev_pair.cuh): pair_kernel<MATH, U, MINB>.
+struct PairVariant {
+  int U, MINB;
+  StepFn fn[2];  // [math mode]
+};
+#define LEV_PAIR_VARIANT(U, M) \
+  { U, M, { pair_kernel<0, U, M>, pair_kernel<1, U, M> } }
+static const PairVariant kPairVariants[] = {
+    LEV_PAIR_VARIANT(8, 3), LEV_PAIR_VARIANT(12, 2), LEV_PAIR_VARIANT(6, 4),
+    LEV_PAIR_VARIANT(16, 2),
+};
+#undef LEV_PAIR_VARIANT
+constexpr int kNumPairVariants = sizeof(kPairVariants) / sizeof(kPairVariants[0]);
+
 // Networks of a batch are grouped by the mean SELL slice length (the
 // per-lane edge count): each class has its own tile list and variant.
 constexpr int kNumClasses = 3;
@@ -86,8 +101,11 @@ struct TileClass {
   int ntiles = 0;
   int tile_off = 0;  // first entry of this class in the tile list
   int variant = 0;
+  int pair_variant = 0;  // two steps per launch with this variant; -1: one
   double mean_len = 0.0;  // mean slice length of the class
   long long edges = 0;
+  float step_ms = 0.0f;  // autotuner: best ms per step, one step per launch
+  float pair_ms = 0.0f;  // autotuner: best ms per step, two steps per launch
 };
 
 // Autotuner results shared by the engines of a process, keyed by the degree
@@ -95,6 +113,7 @@ struct TileClass {
 // (power-of-two bucket).
 static std::mutex g_tune_mu;
 static std::map<std::tuple<int, int, int>, int> g_tune_cache;
+static std::map<std::tuple<int, int, int>, int> g_pair_cache;
 
 inline std::tuple<int, int, int> tune_key(const TileClass &tc, int c) {
   int bucket = 0;
@@ -138,6 +157,11 @@ struct LevEngine {
   float *d_omega_hat = nullptr;
   float *d_ring = nullptr;
   float2 *d_part = nullptr;
+
+  // two steps per launch (lev_pair.cuh): possible when no delay is 0
+  bool pair_ok = false;
+  bool use_pairs = true;
+  float2 *d_pend = nullptr;  // [total_nodes] parked (coupling sum, eps)
 
   // r of the last single step, written by the kernel into mapped host memory
   float *h_rmap = nullptr;
@@ -201,6 +225,7 @@ void free_engine(LevEngine *h) {
   cudaFree(h->d_omega_hat);
   cudaFree(h->d_ring);
   cudaFree(h->d_part);
+  cudaFree(h->d_pend);
   cudaFree(h->d_rhist);
   if (h->h_rmap) cudaFreeHost(h->h_rmap);
   if (h->h_rstage) cudaFreeHost(h->h_rstage);
@@ -288,6 +313,7 @@ StepArgs make_args(LevEngine *h, float dt, float *r_hist, int r_cap,
   a.num_nets = h->num_nets;
   a.dt = dt;
   a.reverse = 0;
+  a.pend = h->d_pend;
   return a;
 }
 
@@ -298,6 +324,12 @@ int prepare_step_kernels() {
     for (int m = 0; m < 2; ++m)
       LEV_TRY_CUDA(cudaFuncSetAttribute(
           reinterpret_cast<const void *>(kVariants[v].fn[m]),
+          cudaFuncAttributePreferredSharedMemoryCarveout,
+          (int)cudaSharedmemCarveoutMaxL1));
+  for (int v = 0; v < kNumPairVariants; ++v)
+    for (int m = 0; m < 2; ++m)
+      LEV_TRY_CUDA(cudaFuncSetAttribute(
+          reinterpret_cast<const void *>(kPairVariants[v].fn[m]),
           cudaFuncAttributePreferredSharedMemoryCarveout,
           (int)cudaSharedmemCarveoutMaxL1));
   return LEV_OK;
@@ -330,6 +362,47 @@ int launch_step(LevEngine *h, StepArgs a) {
   return LEV_OK;
 }
 
+// Two-steps-per-launch path (lev_pair.cuh) in use for at least one class.
+bool pairs_active(const LevEngine *h) {
+  if (!h->pair_ok || !h->use_pairs) return false;
+  for (int c = 0; c < kNumClasses; ++c)
+    if (h->classes[c].ntiles > 0 && h->classes[c].pair_variant >= 0) return true;
+  return false;
+}
+
+// phase 0: pair_kernel (or a first step_kernel for a class without a pair
+// variant); phase 1: finish_kernel (or a second step_kernel).
+int launch_pair_class(LevEngine *h, int c, StepArgs a, int phase) {
+  const TileClass &tc = h->classes[c];
+  if (tc.ntiles == 0) return LEV_OK;
+  a.tiles = h->d_tiles + tc.tile_off;
+  const int mode = (h->math_mode == LEV_MATH_ACCURATE) ? 1 : 0;
+  const void *fn;
+  if (tc.pair_variant < 0)
+    fn = reinterpret_cast<const void *>(kVariants[tc.variant].fn[mode]);
+  else if (phase == 0)
+    fn = reinterpret_cast<const void *>(kPairVariants[tc.pair_variant].fn[mode]);
+  else
+    fn = mode ? reinterpret_cast<const void *>(finish_kernel<1>)
+              : reinterpret_cast<const void *>(finish_kernel<0>);
+  void *args[] = {&a};
+  LEV_TRY_CUDA(cudaLaunchKernel(fn, dim3(tc.ntiles), dim3(kTile), args, 0, h->stream));
+  return LEV_OK;
+}
+
+// Two steps of every class.
+int launch_two_steps(LevEngine *h, StepArgs a) {
+  for (int phase = 0; phase < 2; ++phase) {
+    a.reverse = h->sweep;
+    h->sweep ^= 1;
+    for (int c = 0; c < kNumClasses; ++c) {
+      int rc = launch_pair_class(h, c, a, phase);
+      if (rc != LEV_OK) return rc;
+    }
+  }
+  return LEV_OK;
+}
+
 void clear_graphs(LevEngine *h) {
   for (auto &kv : h->graphs) {
     if (kv.second.exec) cudaGraphExecDestroy(kv.second.exec);
@@ -355,7 +428,16 @@ int get_graph(LevEngine *h, int len, float dt, cudaGraphExec_t *out) {
   reset_rpos_kernel<<<1, 128, 0, h->stream>>>(h->d_st, h->num_nets);
   StepArgs a = make_args(h, dt, h->d_rhist, h->block_len, nullptr);
   int rc = LEV_OK;
-  for (int i = 0; i < len && rc == LEV_OK; ++i) rc = launch_step(h, a);
+  const bool pairs = pairs_active(h);
+  for (int i = 0; i < len && rc == LEV_OK;) {
+    if (pairs && i + 1 < len) {
+      rc = launch_two_steps(h, a);
+      i += 2;
+    } else {
+      rc = launch_step(h, a);
+      i += 1;
+    }
+  }
   cudaError_t ce = cudaStreamEndCapture(h->stream, &ge.graph);
   if (rc != LEV_OK) {
     if (ge.graph) cudaGraphDestroy(ge.graph);
@@ -670,6 +752,8 @@ int create_impl(LevEngine **out, int num_nets, const int32_t *Ns,
     for (int c = 0; c < kNumClasses; ++c) {
       auto it = g_tune_cache.find(tune_key(h->classes[c], c));
       h->classes[c].variant = (it != g_tune_cache.end()) ? it->second : 0;
+      auto ip = g_pair_cache.find(tune_key(h->classes[c], c));
+      h->classes[c].pair_variant = (ip != g_pair_cache.end()) ? ip->second : 0;
     }
   }
 
@@ -805,6 +889,7 @@ int create_impl(LevEngine **out, int num_nets, const int32_t *Ns,
       return cleanup_fail(LEV_ERR_ARG, "col_idx out of range [0, N)");
     if (herr & 2u)
       return cleanup_fail(LEV_ERR_ARG, "delay larger than max_delay");
+    h->pair_ok = !(herr & 4u);
     cudaFree(d_tmp);
     cudaFree(d_tcol);
     cudaFree(d_tw);
@@ -815,6 +900,15 @@ int create_impl(LevEngine **out, int num_nets, const int32_t *Ns,
     d_err = nullptr;
   }
 #undef LEV_UP
+  if (edge_off == 0) h->pair_ok = true;
+  if (h->pair_ok) {
+    int r2 = dev_alloc(h, &h->d_pend, (size_t)node_off);
+    if (r2 != LEV_OK) {
+      std::string msg = g_last_error;
+      free_engine(h);
+      return fail(r2, msg);
+    }
+  }
   for (int n = 0; n < num_nets; ++n) {
     int r2 = launch_fill(h, n);
     if (r2 != LEV_OK) {
@@ -1335,6 +1429,53 @@ int lev_set_cluster_mode(LevEngine *h, int32_t enabled) {
 
 int lev_num_variants(void) { return kNumVariants; }
 
+int lev_num_pair_variants(void) { return kNumPairVariants; }
+
+int lev_pair_variant_info(int32_t v, int32_t *unroll, int32_t *min_blocks) {
+  if (v < 0 || v >= kNumPairVariants) return fail(LEV_ERR_ARG, "pair variant out of range");
+  if (unroll) *unroll = kPairVariants[v].U;
+  if (min_blocks) *min_blocks = kPairVariants[v].MINB;
+  return LEV_OK;
+}
+
+int lev_pair_info(const LevEngine *h, int32_t c, int32_t *eligible, int32_t *enabled,
+                  int32_t *pair_variant, float *pair_ms, float *step_ms) {
+  if (!h) return fail(LEV_ERR_ARG, "null handle");
+  if (c < 0 || c >= kNumClasses) return fail(LEV_ERR_ARG, "class out of range");
+  const TileClass &tc = h->classes[c];
+  if (eligible) *eligible = h->pair_ok ? 1 : 0;
+  if (enabled) *enabled = pairs_active(h) ? 1 : 0;
+  if (pair_variant) *pair_variant = tc.pair_variant;
+  if (pair_ms) *pair_ms = tc.pair_ms;
+  if (step_ms) *step_ms = tc.step_ms;
+  return LEV_OK;
+}
+
+int lev_set_pair_mode(LevEngine *h, int32_t enabled) {
+  if (!h) return fail(LEV_ERR_ARG, "null handle");
+  if ((enabled != 0) != h->use_pairs) {
+    DeviceScope ds(h->device);
+    cudaStreamSynchronize(h->stream);
+    clear_graphs(h);
+    h->use_pairs = enabled != 0;
+  }
+  return LEV_OK;
+}
+
+int lev_set_pair_variant(LevEngine *h, int32_t c, int32_t v) {
+  if (!h) return fail(LEV_ERR_ARG, "null handle");
+  if (c < 0 || c >= kNumClasses) return fail(LEV_ERR_ARG, "class out of range");
+  if (v < -1 || v >= kNumPairVariants)
+    return fail(LEV_ERR_ARG, "pair variant out of range (-1 turns pairs off)");
+  if (h->classes[c].pair_variant != v) {
+    DeviceScope ds(h->device);
+    cudaStreamSynchronize(h->stream);
+    clear_graphs(h);
+    h->classes[c].pair_variant = v;
+  }
+  return LEV_OK;
+}
+
 int lev_variant_info(int32_t v, int32_t *unroll, int32_t *pipelined,
                      int32_t *min_blocks) {
   if (v < 0 || v >= kNumVariants) return fail(LEV_ERR_ARG, "variant out of range");
@@ -1463,9 +1604,46 @@ int lev_autotune(LevEngine *h, float dt, int32_t trial_steps,
       }
     }
     tc.variant = best_v;
+    tc.step_ms = best;
     if (variant_out) variant_out[c] = best_v;
+    // two steps per launch: pair_kernel + finish_kernel per two steps; kept
+    // for this class only where it beats the best one-step variant
+    if (h->pair_ok && rc == LEV_OK) {
+      const int pairs = std::max(1, trial_steps / 2);
+      float best_p = 0.0f;
+      int best_pv = -1;
+      for (int v = 0; v < kNumPairVariants && rc == LEV_OK; ++v) {
+        tc.pair_variant = v;
+        for (int ph = 0; ph < 2 && rc == LEV_OK; ++ph) {  // warm-up
+          a.reverse = ph;
+          rc = launch_pair_class(h, c, a, ph);
+        }
+        if (rc != LEV_OK) break;
+        cudaEventRecord(e0, h->stream);
+        for (int i = 0; i < pairs && rc == LEV_OK; ++i)
+          for (int ph = 0; ph < 2 && rc == LEV_OK; ++ph) {
+            a.reverse = ph;
+            rc = launch_pair_class(h, c, a, ph);
+          }
+        cudaEventRecord(e1, h->stream);
+        if (cudaEventSynchronize(e1) != cudaSuccess) {
+          rc = fail(LEV_ERR_CUDA, "autotune: pair trial failed");
+          break;
+        }
+        float ms = 0.0f;
+        cudaEventElapsedTime(&ms, e0, e1);
+        ms /= 2.0f * pairs;
+        if (best_pv < 0 || ms < best_p) {
+          best_p = ms;
+          best_pv = v;
+        }
+      }
+      tc.pair_ms = best_p;
+      tc.pair_variant = (best_pv >= 0 && best_p < best) ? best_pv : -1;
+    }
     std::lock_guard<std::mutex> lk(g_tune_mu);
     g_tune_cache[tune_key(tc, c)] = best_v;
+    if (h->pair_ok) g_pair_cache[tune_key(tc, c)] = tc.pair_variant;
   }
   // small single networks: cluster-resident kernel or per-step graph replay
   if (rc == LEV_OK && h->cluster_ok) {

@@ -107,6 +107,7 @@ struct StepArgs {
   int num_nets;
   float dt;
   int reverse;  // 1: CTAs walk the tile list backwards (alternating sweeps)
+  float2 *pend;  // [nodes] (coupling sum, eps) of a half-done step (lev_pair.cuh)
 };
 
 // ---------------------------------------------------------------------------
@@ -421,7 +422,8 @@ __global__ void ring_fill_kernel(const float *__restrict__ theta,
 // CSR -> SELL-32 for one network: entry k of row i goes to
 // sl_off[slice_base + i/32] + 32k + i%32.  One thread per row.
 // mode 0: pack (col, delay) into sl_cd and copy weights, validating
-//         col in [0,N) and delay <= max_delay (bits of *err);
+//         col in [0,N) and delay <= max_delay (bits 1, 2 of *err); bit 4
+//         reports a zero delay;
 // mode 1: weights only, CSR -> SELL;   mode 2: weights only, SELL -> CSR.
 __global__ void sell_convert_kernel(int mode, const int *__restrict__ row_ptr,
                                     int N, long long slice_base,
@@ -444,6 +446,7 @@ __global__ void sell_convert_kernel(int mode, const int *__restrict__ row_ptr,
         const int d = delays[e];
         if (c < 0 || c >= N) bad |= 1u;
         if (d > max_delay) bad |= 2u;
+        if (d == 0) bad |= 4u;  // not an error: rules out two steps per launch
         sl_cd[idx] = ((uint32_t)c << 8) | (uint32_t)d;
         sl_w[idx] = w_csr[e];
       } else if (mode == 1) {

@@ -283,6 +283,33 @@ class _EngineBase:
     def set_cluster_mode(self, enabled: bool) -> None:
         check(self._lib.lev_set_cluster_mode(self.handle, 1 if enabled else 0))
 
+    # -- two steps per launch (step blocks; no zero delays) -----------------
+    def pair_info(self) -> list:
+        """Per degree class: whether two steps per launch are possible
+        (eligible: no zero delay) and in use, the pair variant (-1: one step
+        per launch for this class) and the autotuner's ms per step of the
+        best pair and one-step variants (0 before autotuning)."""
+        out = []
+        for c in range(3):
+            el, en, pv = C.c_int32(), C.c_int32(), C.c_int32()
+            pms, sms = C.c_float(), C.c_float()
+            check(self._lib.lev_pair_info(self.handle, c, C.byref(el), C.byref(en),
+                                          C.byref(pv), C.byref(pms), C.byref(sms)))
+            info = dict(cls=c, eligible=bool(el.value), enabled=bool(en.value),
+                        pair_variant=pv.value, pair_ms=pms.value, step_ms=sms.value)
+            if pv.value >= 0:
+                u, m = C.c_int32(), C.c_int32()
+                check(self._lib.lev_pair_variant_info(pv.value, C.byref(u), C.byref(m)))
+                info.update(unroll=u.value, min_blocks=m.value)
+            out.append(info)
+        return out
+
+    def set_pair_mode(self, enabled: bool) -> None:
+        check(self._lib.lev_set_pair_mode(self.handle, 1 if enabled else 0))
+
+    def set_pair_variant(self, cls: int, variant: int) -> None:
+        check(self._lib.lev_set_pair_variant(self.handle, int(cls), int(variant)))
+
     # -- checkpoint ---------------------------------------------------------
     def get_state(self) -> dict:
         """Full engine state (the reference exposes no such getter)."""

@@ -93,6 +93,66 @@ def test_engine_bit_identical_to_reference_golden(case):
         np.testing.assert_array_equal(np.asarray(got), z[key], err_msg=key)
 
 
+def _replay_blocks(e, actions, record, dt):
+    """make_golden.replay with every run of steps between two recorded
+    points taken as one step block (lev_step_n: graph replay, two steps per
+    launch where the network has no zero delay)."""
+    rs, out, t = [], {}, 0
+    points = sorted(set().union(*record.values()))
+    for act in actions:
+        kind = act[0]
+        if kind == "step":
+            end = t + act[1]
+            while t < end:
+                nxt = min([p for p in points if t < p <= end] or [end])
+                rs.append(e.step_n(dt, nxt - t))
+                t = nxt
+                if t in points:
+                    th_hat, om_hat = e.get_predictor()
+                    ring, bi = e.get_ring(0)
+                    snap = dict(theta=e.get_theta(), weights=e.get_weights(),
+                                theta_hat=th_hat, omega_hat=om_hat, ring=ring,
+                                buf_idx=np.int32(bi))
+                    for key, names in (("theta", ["theta"]), ("weights", ["weights"]),
+                                       ("predictor", ["theta_hat", "omega_hat"]),
+                                       ("ring", ["ring", "buf_idx"])):
+                        if t in record.get(key, ()):
+                            for nm in names:
+                                out[f"{nm}@{t}"] = snap[nm]
+                    out[f"g@{t}"] = np.float32(e.get_gain())
+        elif kind == "set_theta":
+            th = e.get_theta()
+            e.set_theta(((th + act[1]) % np.float32(2 * np.pi)).astype(np.float32))
+        elif kind == "set_theta_raw":
+            th = e.get_theta().copy()
+            m = act[1] != 0
+            th[m] = act[1][m]
+            e.set_theta(th.astype(np.float32))
+        elif kind == "set_gain":
+            e.set_gain(act[1])
+        elif kind == "controller":
+            e.set_gain_controller(act[1])
+    return np.concatenate(rs).astype(np.float32), out
+
+
+@pytest.mark.skipif(not golden_cases(), reason="golden vectors not generated")
+@pytest.mark.parametrize("case", golden_cases() or ["none"])
+def test_step_blocks_bit_identical_to_reference_golden(case):
+    """Step blocks (graph replay; two steps per launch where no delay is 0)
+    reproduce the reference engine bit for bit, including blocks of odd
+    length and blocks interrupted by set_theta / gain / controller calls."""
+    z = load_golden(case)
+    net = network_from_golden(z)
+    e = LeviathanEngine(*net.engine_args())
+    e.set_cluster_mode(False)
+    assert e.pair_info()[0]["eligible"] == bool(np.all(net.delays > 0))
+    rs, snaps = _replay_blocks(e, decode_actions(z), record_from_golden(z), float(z["dt"]))
+    e.close()
+    np.testing.assert_array_equal(rs, z["r"])
+    for key, got in snaps.items():
+        np.testing.assert_array_equal(np.asarray(got), z[key], err_msg=key)
+
+
 def test_division_free_wraps_are_bitwise_ieee_for_all_inputs():
     """The phase wraps evaluated without a division equal the reference's
     IEEE-division expressions (leviathan_kernel.cu:105,146,188) in every bit,
@@ -257,6 +317,77 @@ def test_autotune_leaves_simulation_unchanged():
             b.set_variant(c, v)
             a.set_variant(c, (v + 1) % len(res["variants"]))
             np.testing.assert_array_equal(a.step_n(DT, 2), b.step_n(DT, 2))
+    a.close()
+    b.close()
+
+
+def _full_state(e):
+    th_hat, om_hat = e.get_predictor()
+    out = dict(theta=e.get_all_theta(), weights=e.get_weights(), theta_hat=th_hat,
+               omega_hat=om_hat)
+    for k in range(e.num_nets):
+        ring, bi = e.get_ring(k)
+        out[f"ring{k}"] = ring
+        out[f"buf{k}"] = np.int64(bi)
+        out[f"g{k}"] = np.float32(e._get_gain(k))
+        out[f"t{k}"] = np.int64(e.step_count(k))
+    return out
+
+
+@pytest.mark.parametrize("mode", ["reference", "accurate"])
+def test_two_steps_per_launch_bit_identical(mode):
+    """Two steps per launch (pair_kernel + finish_kernel) against one step
+    per launch: every pair variant, a single network at scale and a batch of
+    uneven networks, odd block lengths, controller on and off."""
+    from leviathan_v1_b200 import _lib
+
+    nvar = _lib.load().lev_num_pair_variants()
+    single = make_network(20_000, 16, 0.1, 30, seed=77)
+    batch = [make_network(n, k, 0.1, md, seed=s)
+             for n, k, md, s in [(700, 8, 10, 1), (2500, 20, 50, 2), (300, 4, 3, 3),
+                                 (4097, 32, 64, 5), (1500, 12, 1, 6)]]
+    params = [dict(g=0.4 * i, gain_controller=i % 2) for i in range(len(batch))]
+    for make in (lambda: LeviathanEngine(*single.engine_args(), math_mode=mode),
+                 lambda: BatchEngine([n.as_dict() for n in batch], params=params,
+                                     math_mode=mode)):
+        ref = make()
+        ref.set_cluster_mode(False)
+        ref.set_pair_mode(False)
+        assert not any(c["enabled"] for c in ref.pair_info())
+        r_ref = np.concatenate([ref.step_n(DT, 3), ref.step_n(DT, 64), ref.step_n(DT, 13)])
+        s_ref = _full_state(ref)
+        ref.close()
+        for v in range(nvar):
+            e = make()
+            if hasattr(e, "set_cluster_mode"):
+                e.set_cluster_mode(False)
+            for c in range(3):
+                e.set_pair_variant(c, v)
+            info = e.pair_info()
+            assert all(c["eligible"] and c["enabled"] for c in info), info
+            r = np.concatenate([e.step_n(DT, 3), e.step_n(DT, 64), e.step_n(DT, 13)])
+            np.testing.assert_array_equal(r, r_ref, err_msg=f"pair variant {v}")
+            for key, want in s_ref.items():
+                np.testing.assert_array_equal(_full_state(e)[key], want,
+                                              err_msg=f"pair variant {v}: {key}")
+            e.close()
+
+
+def test_zero_delay_takes_one_step_per_launch():
+    """A zero delay reads theta_j(t+1) in step t+1, which another CTA writes
+    in the same launch: such engines are not eligible and step blocks take
+    one step per launch (still equal to repeated single steps)."""
+    net = make_network(3000, 12, 0.1, 6, seed=12, delay_lo=0)
+    assert (net.delays == 0).any()
+    a = LeviathanEngine(*net.engine_args())
+    b = LeviathanEngine(*net.engine_args())
+    a.set_cluster_mode(False)
+    info = a.pair_info()
+    assert not info[0]["eligible"] and not info[0]["enabled"]
+    ra = a.step_n(DT, 41)
+    rb = np.array([b.step(DT) for _ in range(41)], np.float32)
+    np.testing.assert_array_equal(ra, rb)
+    np.testing.assert_array_equal(a.get_theta(), b.get_theta())
     a.close()
     b.close()
 
