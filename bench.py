@@ -13,8 +13,14 @@ Metric: edge-updates/s = E x steps / elapsed.
 * ``value``   -- device-resident throughput: K steps replayed from CUDA
   graphs, timed with CUDA events on the engine stream, max over ranks.
 * ``e2e``     -- the whole job through the public API with host buffers:
-  ``LeviathanEngine(...)`` from host arrays (H2D), K x ``step(dt)`` each
-  returning r to the host, ``get_theta()`` (D2H), wall clock.
+  ``LeviathanEngine(...)`` from host arrays (H2D), ``step_n(dt, K)``
+  returning r of every step to the host (the block form
+  ``LeviathanObservatory.run_baseline`` uses), ``get_theta()`` (D2H), wall
+  clock; ``e2e.per_step_calls`` is the same job with K x ``step(dt)``.
+* ``roofline`` -- the dominant kernel (two steps per launch: pair_kernel) at
+  its algorithmic bytes per launch over its mean launch duration (CUDA
+  events on the engine stream), against the measured HBM copy peak; the
+  per-step figure of the whole launch sequence is in ``step_sequence``.
 * ``--impl reference`` runs the reference engine itself (its
   leviathan_kernel.cu built from the reference sources for sm_100a, and its
   stock 86;90 build, in oracle/_ref) through its C ABI on the same GPU, the
@@ -114,8 +120,8 @@ def measured_peaks():
 
 
 def profiled_traffic(kernel="step_kernel"):
-    """DRAM bytes per launch of the step kernel from the committed ncu
-    summary (profiles/), or None."""
+    """DRAM bytes per launch of ``kernel`` on this workload from the
+    committed ncu summary (profiles/<kernel>_traffic.txt), or None."""
     path = os.path.join(REPO, "profiles", f"{kernel}_traffic.txt")
     if not os.path.exists(path):
         return None
@@ -189,6 +195,18 @@ def build_workload(seed):
 
     return make_network(WORKLOAD["N"], WORKLOAD["k"], WORKLOAD["p"],
                         WORKLOAD["max_delay"], seed)
+
+
+def launches_per_job(K, pairs, block=256):
+    """Kernel launches of K steps run as step blocks of `block` steps (one
+    graph each): a reset of the r-history counter per block, then per two
+    steps pair_kernel, reduce_kernel, finish_kernel, reduce_kernel -- or one
+    step_kernel per step."""
+    n = 0
+    for b0 in range(0, K, block):
+        L = min(block, K - b0)
+        n += 1 + ((L // 2) * 4 + (L % 2) if pairs else L)
+    return n
 
 
 def algorithmic_bytes(N, E):
@@ -433,8 +451,8 @@ def run_ours(args, rank, world, local):
     # the in-project autotuner picks the step-kernel variant for this degree
     # distribution (state is restored; later engines of the process reuse it)
     tune = eng.autotune(DT, trial_steps=10)
-    pair_info = [c for c in eng.pair_info() if c["cls"] == max(tune["chosen"]) or True]
-    pair_info = [c for c, t in zip(eng.pair_info(), eng.tuning()) if t["tiles"]]
+    cls = next(t["cls"] for t in eng.tuning() if t["tiles"])
+    pair_info = eng.pair_info()[cls]
     stream = torch.cuda.ExternalStream(eng.stream_ptr)
     sampler = ClockSampler(torch.cuda.current_device()).start()
 
@@ -459,32 +477,63 @@ def run_ours(args, rank, world, local):
     edges_total = sum_over_ranks(E, world)
     value = edges_total * K / (ms_max / 1e3)
     r_last = eng.get_r()
+    # launch durations of the dominant kernel (CUDA events on the engine
+    # stream; pair_kernel, then finish_kernel, of a two-step round)
+    t_launch = eng.time_launches(DT, 20)
     eng.close()
 
-    # end-to-end through the public API with host buffers
+    # end-to-end through the public API with host buffers: construction from
+    # host arrays, K steps with r of every step returned to the host (the
+    # block form used by LeviathanObservatory.run_baseline), final phases
+    h2d = (N + 1) * 4 + E * (4 + 1 + 4) + N * 4 * 3
+    d2h = 4 * K + 4 * N
     barrier(world)
     torch.cuda.synchronize()
     t0 = time.perf_counter()
     e2 = LeviathanEngine(*net.engine_args())
-    for _ in range(K):
-        e2.step(DT)
+    r_hist = e2.step_n(DT, K)
     theta = e2.get_theta()
     torch.cuda.synchronize()
     e2e_s = time.perf_counter() - t0
     e2.close()
     e2e_s = max_over_ranks(e2e_s, world)
-    h2d = (N + 1) * 4 + E * (4 + 1 + 4) + N * 4 * 3
-    d2h = 4 * K + 4 * N
+    # the same job with one step(dt) call per step (reference call pattern)
+    barrier(world)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    e3 = LeviathanEngine(*net.engine_args())
+    for _ in range(K):
+        e3.step(DT)
+    e3.get_theta()
+    torch.cuda.synchronize()
+    e3_s = max_over_ranks(time.perf_counter() - t0, world)
+    e3.close()
     e2e = {"value": edges_total * K / e2e_s, "unit": "edge-updates/s",
            "h2d_bytes_per_step": h2d / K, "d2h_bytes_per_step": d2h / K,
-           "path": "LeviathanEngine(host arrays) + K x step(dt)->r + get_theta()",
-           "seconds": e2e_s}
+           "path": "LeviathanEngine(host arrays) + step_n(dt, K) -> r[K] + get_theta()",
+           "seconds": e2e_s,
+           "per_step_calls": {"value": edges_total * K / e3_s, "seconds": e3_s,
+                              "path": "LeviathanEngine(host arrays) + K x step(dt) -> r "
+                                      "+ get_theta()"}}
 
     step_s = ms / 1e3 / K
     alg = algorithmic_bytes(N, E)
     peak, peak_kind = measured_peaks()
-    achieved = alg / step_s / 1e9
-    traffic = profiled_traffic()
+    pairs = pair_info["enabled"] and pair_info["pair_variant"] >= 0
+    if pairs:
+        # pair_kernel: two steps' edge work, 2 x 17 B per edge; per node
+        # row_ptr 4, theta r/w 8, theta_hat r/w 8, omega_hat r/w 8, omega 4,
+        # ring write 4, parked (sum, eps) write 8 = 44 B
+        kernel = "lev::pair_kernel (steps t and t+1 but the last integrate)"
+        alg_launch = 34 * E + 44 * N + 4
+        launch_s = t_launch[0] / 1e3
+        traffic = profiled_traffic("pair_kernel")
+    else:
+        kernel = "lev::step_kernel"
+        alg_launch = alg
+        launch_s = t_launch[0] / 1e3
+        traffic = profiled_traffic("step_kernel")
+    achieved = alg_launch / launch_s / 1e9
     line = {
         "metric": "edge-updates/s", "value": value, "unit": "edge-updates/s",
         "n_gpus": world, "steps": K, "warmup": W, "ms_per_step": ms_max / K,
@@ -496,12 +545,17 @@ def run_ours(args, rank, world, local):
                    "l2": "inputs (1.2 GB) larger than L2 (126 MB); no flush"},
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak,
                      "unit": "GB/s", "frac": achieved / peak, "peak_kind": peak_kind,
-                     "traffic": traffic, "kernel": "lev::step_kernel<0,...>",
-                     "algorithmic_bytes_per_launch": alg,
-                     "variant": tune["variants"][max(tune["chosen"])] if tune else None,
-                     "two_steps_per_launch": pair_info[0]},
+                     "traffic": traffic, "kernel": kernel,
+                     "algorithmic_bytes_per_launch": alg_launch,
+                     "launch_us": t_launch[0] * 1e3,
+                     "second_launch_us": t_launch[1] * 1e3,
+                     "step_sequence": {"algorithmic_bytes_per_step": alg,
+                                       "achieved": alg / step_s / 1e9,
+                                       "frac": alg / step_s / 1e9 / peak},
+                     "one_step_variant": tune["variants"][tune["chosen"][cls]],
+                     "two_steps_per_launch": pair_info},
         "e2e": e2e,
-        "gpu_launches": K + (K + 255) // 256,
+        "gpu_launches": launches_per_job(K, pairs),
         "clocks": clocks,
         "r_final": r_last,
         "theta_finite": bool(np.all(np.isfinite(theta))),

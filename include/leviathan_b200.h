@@ -250,18 +250,28 @@ int lev_set_cluster_mode(LevEngine *h, int32_t enabled);
  * (lev_step_n / lev_step_n_async) walk each row's edges for steps t and t+1
  * in one launch and finish step t+1's integrate, which needs the gain
  * g(t+1) and so the global r(t+1), in a short node-only launch.  The
- * edge streams then leave HBM once per two steps.  Results are bitwise those
- * of one step per launch.  lev_autotune times the pair variants of each
+ * edge streams then leave HBM once per two steps.  `deep` variants keep two
+ * groups of edges in flight per lane.
+ * Results are bitwise those of one step per launch.  lev_autotune times the pair variants of each
  * degree class against its best one-step variant and keeps pairs only where
  * they are faster; pair_variant -1 means one step per launch for that class.
  * lev_step (single steps, and the reference ABI) always takes one step per
  * launch. */
 int lev_num_pair_variants(void);
-int lev_pair_variant_info(int32_t v, int32_t *unroll, int32_t *min_blocks);
+int lev_pair_variant_info(int32_t v, int32_t *unroll, int32_t *min_blocks,
+                          int32_t *deep);
 int lev_pair_info(const LevEngine *h, int32_t c, int32_t *eligible, int32_t *enabled,
                   int32_t *pair_variant, float *pair_ms, float *step_ms);
 int lev_set_pair_mode(LevEngine *h, int32_t enabled);
 int lev_set_pair_variant(LevEngine *h, int32_t c, int32_t v);
+
+/* Launch durations for profiling (no reference counterpart): runs n rounds
+ * of two launch phases on the engine stream, each bracketed by CUDA events,
+ * and advances the simulation by 2n steps.  With two steps per launch in use
+ * ms_out[0] is the mean duration of the pair_kernel phase and ms_out[1] of
+ * the finish_kernel phase; otherwise both are one-step launches.  (All
+ * degree classes launch within a phase.) */
+int lev_time_launches(LevEngine *h, float dt, int32_t n, float *ms_out);
 
 /* Times every variant on every non-empty class of this engine
  * (trial_steps steps each, after two warm-up steps), keeps the fastest per

@@ -103,11 +103,13 @@ PROTOTYPES = {
                                    C.POINTER(_i32), C.POINTER(_i32), C.POINTER(_i64)]),
     "lev_set_cluster_mode": (C.c_int, [_P, _i32]),
     "lev_num_pair_variants": (C.c_int, []),
-    "lev_pair_variant_info": (C.c_int, [_i32, C.POINTER(_i32), C.POINTER(_i32)]),
+    "lev_pair_variant_info": (C.c_int, [_i32, C.POINTER(_i32), C.POINTER(_i32),
+                                        C.POINTER(_i32)]),
     "lev_pair_info": (C.c_int, [_P, _i32, C.POINTER(_i32), C.POINTER(_i32),
                                 C.POINTER(_i32), C.POINTER(_f32), C.POINTER(_f32)]),
     "lev_set_pair_mode": (C.c_int, [_P, _i32]),
     "lev_set_pair_variant": (C.c_int, [_P, _i32, _i32]),
+    "lev_time_launches": (C.c_int, [_P, _f32, _i32, _P]),
     "lev_num_variants": (C.c_int, []),
     "lev_variant_info": (C.c_int, [_i32, C.POINTER(_i32), C.POINTER(_i32),
                                    C.POINTER(_i32)]),

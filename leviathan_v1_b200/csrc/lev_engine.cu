@@ -76,16 +76,20 @@ static const StepVariant kVariants[] = {
 #undef LEV_VARIANT
 constexpr int kNumVariants = sizeof(kVariants) / sizeof(kVariants[0]);
 
-// Two-steps-per-launch variants (lev_pair.cuh): pair_kernel<MATH, U, MINB>.
+// Two-steps-per-launch variants (lev_pair.cuh): pair_kernel<MATH, U, MINB,
+// DEEP> (DEEP: two-stage software pipeline).  Measured on B200: fewer
+// resident CTAs with more loads in flight per lane win at large networks
+// (the L1 keeps the tile's ring lines and col/delay words between the two
+// walks); more CTAs win at the small networks of a sweep.
 struct PairVariant {
-  int U, MINB;
+  int U, MINB, DEEP;
   StepFn fn[2];  // [math mode]
 };
-#define LEV_PAIR_VARIANT(U, M) \
-  { U, M, { pair_kernel<0, U, M>, pair_kernel<1, U, M> } }
+#define LEV_PAIR_VARIANT(U, M, D) \
+  { U, M, D, { pair_kernel<0, U, M, D>, pair_kernel<1, U, M, D> } }
 static const PairVariant kPairVariants[] = {
-    LEV_PAIR_VARIANT(8, 3), LEV_PAIR_VARIANT(12, 2), LEV_PAIR_VARIANT(6, 4),
-    LEV_PAIR_VARIANT(16, 2),
+    LEV_PAIR_VARIANT(8, 2, 1), LEV_PAIR_VARIANT(6, 3, 1), LEV_PAIR_VARIANT(8, 3, 0),
+    LEV_PAIR_VARIANT(4, 4, 1), LEV_PAIR_VARIANT(10, 2, 1),
 };
 #undef LEV_PAIR_VARIANT
 constexpr int kNumPairVariants = sizeof(kPairVariants) / sizeof(kPairVariants[0]);
@@ -104,6 +108,8 @@ struct TileClass {
   int pair_variant = 0;  // two steps per launch with this variant; -1: one
   double mean_len = 0.0;  // mean slice length of the class
   long long edges = 0;
+  int net_off = 0;       // first entry of this class in the class network list
+  int nnets = 0;
   float step_ms = 0.0f;  // autotuner: best ms per step, one step per launch
   float pair_ms = 0.0f;  // autotuner: best ms per step, two steps per launch
 };
@@ -162,6 +168,7 @@ struct LevEngine {
   bool pair_ok = false;
   bool use_pairs = true;
   float2 *d_pend = nullptr;  // [total_nodes] parked (coupling sum, eps)
+  int *d_class_nets = nullptr;  // networks of each class, class by class
 
   // r of the last single step, written by the kernel into mapped host memory
   float *h_rmap = nullptr;
@@ -226,6 +233,7 @@ void free_engine(LevEngine *h) {
   cudaFree(h->d_ring);
   cudaFree(h->d_part);
   cudaFree(h->d_pend);
+  cudaFree(h->d_class_nets);
   cudaFree(h->d_rhist);
   if (h->h_rmap) cudaFreeHost(h->h_rmap);
   if (h->h_rstage) cudaFreeHost(h->h_rstage);
@@ -362,6 +370,9 @@ int launch_step(LevEngine *h, StepArgs a) {
   return LEV_OK;
 }
 
+// A pair variant index in range.
+bool pair_variant_ok(const LevEngine *, int v) { return v >= 0 && v < kNumPairVariants; }
+
 // Two-steps-per-launch path (lev_pair.cuh) in use for at least one class.
 bool pairs_active(const LevEngine *h) {
   if (!h->pair_ok || !h->use_pairs) return false;
@@ -377,16 +388,25 @@ int launch_pair_class(LevEngine *h, int c, StepArgs a, int phase) {
   if (tc.ntiles == 0) return LEV_OK;
   a.tiles = h->d_tiles + tc.tile_off;
   const int mode = (h->math_mode == LEV_MATH_ACCURATE) ? 1 : 0;
-  const void *fn;
-  if (tc.pair_variant < 0)
-    fn = reinterpret_cast<const void *>(kVariants[tc.variant].fn[mode]);
-  else if (phase == 0)
-    fn = reinterpret_cast<const void *>(kPairVariants[tc.pair_variant].fn[mode]);
-  else
-    fn = mode ? reinterpret_cast<const void *>(finish_kernel<1>)
-              : reinterpret_cast<const void *>(finish_kernel<0>);
-  void *args[] = {&a};
-  LEV_TRY_CUDA(cudaLaunchKernel(fn, dim3(tc.ntiles), dim3(kTile), args, 0, h->stream));
+  if (tc.pair_variant < 0 || phase == 0) {
+    const void *fn =
+        tc.pair_variant < 0
+            ? reinterpret_cast<const void *>(kVariants[tc.variant].fn[mode])
+            : reinterpret_cast<const void *>(kPairVariants[tc.pair_variant].fn[mode]);
+    void *args[] = {&a};
+    LEV_TRY_CUDA(cudaLaunchKernel(fn, dim3(tc.ntiles), dim3(kTile), args, 0, h->stream));
+  } else {
+    const int blocks = (tc.ntiles + kFinishTiles - 1) / kFinishTiles;
+    if (mode)
+      finish_kernel<1><<<blocks, kTile, 0, h->stream>>>(a, tc.ntiles);
+    else
+      finish_kernel<0><<<blocks, kTile, 0, h->stream>>>(a, tc.ntiles);
+    LEV_TRY_CUDA(cudaGetLastError());
+  }
+  if (tc.pair_variant >= 0) {  // r and g of the class's networks
+    reduce_kernel<<<tc.nnets, kReduceThreads, 0, h->stream>>>(a, h->d_class_nets + tc.net_off);
+    LEV_TRY_CUDA(cudaGetLastError());
+  }
   return LEV_OK;
 }
 
@@ -736,6 +756,13 @@ int create_impl(LevEngine **out, int num_nets, const int32_t *Ns,
   }
   for (int c = 1; c < kNumClasses; ++c)
     h->classes[c].tile_off = h->classes[c - 1].tile_off + h->classes[c - 1].ntiles;
+  std::vector<int> h_class_nets;
+  for (int c = 0; c < kNumClasses; ++c) {
+    h->classes[c].net_off = (int)h_class_nets.size();
+    for (int n = 0; n < num_nets; ++n)
+      if (net_class[n] == c) h_class_nets.push_back(n);
+    h->classes[c].nnets = (int)h_class_nets.size() - h->classes[c].net_off;
+  }
   std::vector<int2> h_tiles(tiles);
   {
     int fill[kNumClasses];
@@ -789,6 +816,7 @@ int create_impl(LevEngine **out, int num_nets, const int32_t *Ns,
   LEV_ALLOC(h->d_ring, (size_t)ring_off);
   LEV_ALLOC(h->d_part, (size_t)tiles);
   LEV_ALLOC(h->d_rhist, (size_t)h->block_len * num_nets);
+  LEV_ALLOC(h->d_class_nets, (size_t)num_nets);
 #undef LEV_ALLOC
   if (rc != LEV_OK) {
     std::string msg = g_last_error;
@@ -829,6 +857,7 @@ int create_impl(LevEngine **out, int num_nets, const int32_t *Ns,
   } while (0)
   LEV_UP(h->d_nets, h->h_nets.data(), sizeof(NetDesc) * num_nets);
   LEV_UP(h->d_tiles, h_tiles.data(), sizeof(int2) * tiles);
+  LEV_UP(h->d_class_nets, h_class_nets.data(), sizeof(int) * num_nets);
   LEV_UP(h->d_row_ptr, rp_cat, sizeof(int32_t) * rp_off);
   LEV_UP(h->d_theta, th_cat, sizeof(float) * node_off);
   LEV_UP(h->d_theta_hat, thh_cat, sizeof(float) * node_off);
@@ -1431,10 +1460,12 @@ int lev_num_variants(void) { return kNumVariants; }
 
 int lev_num_pair_variants(void) { return kNumPairVariants; }
 
-int lev_pair_variant_info(int32_t v, int32_t *unroll, int32_t *min_blocks) {
+int lev_pair_variant_info(int32_t v, int32_t *unroll, int32_t *min_blocks,
+                          int32_t *deep) {
   if (v < 0 || v >= kNumPairVariants) return fail(LEV_ERR_ARG, "pair variant out of range");
   if (unroll) *unroll = kPairVariants[v].U;
   if (min_blocks) *min_blocks = kPairVariants[v].MINB;
+  if (deep) *deep = kPairVariants[v].DEEP;
   return LEV_OK;
 }
 
@@ -1473,6 +1504,46 @@ int lev_set_pair_variant(LevEngine *h, int32_t c, int32_t v) {
     clear_graphs(h);
     h->classes[c].pair_variant = v;
   }
+  return LEV_OK;
+}
+
+int lev_time_launches(LevEngine *h, float dt, int32_t n, float *ms_out) {
+  if (!h || !ms_out) return fail(LEV_ERR_ARG, "null argument");
+  if (n < 1) return fail(LEV_ERR_ARG, "n must be >= 1");
+  if (!std::isfinite(dt)) return fail(LEV_ERR_ARG, "dt is not finite");
+  DeviceScope ds(h->device);
+  const bool pairs = pairs_active(h);
+  cudaEvent_t ev[3] = {nullptr, nullptr, nullptr};
+  int rc = LEV_OK;
+  for (int i = 0; i < 3 && rc == LEV_OK; ++i)
+    if (cudaEventCreate(&ev[i]) != cudaSuccess) rc = fail(LEV_ERR_CUDA, "event creation failed");
+  StepArgs a = make_args(h, dt, nullptr, 0, nullptr);
+  double sum[2] = {0.0, 0.0};
+  for (int i = 0; i < n && rc == LEV_OK; ++i) {
+    float ms0 = 0.0f, ms1 = 0.0f;
+    for (int phase = 0; phase < 2 && rc == LEV_OK; ++phase) {
+      cudaEventRecord(ev[phase], h->stream);
+      a.reverse = h->sweep;
+      h->sweep ^= 1;
+      for (int c = 0; c < kNumClasses && rc == LEV_OK; ++c)
+        rc = pairs ? launch_pair_class(h, c, a, phase) : launch_class(h, c, a);
+    }
+    cudaEventRecord(ev[2], h->stream);
+    if (rc != LEV_OK) break;
+    if (cudaEventSynchronize(ev[2]) != cudaSuccess) {
+      rc = fail(LEV_ERR_CUDA, "timed launches failed");
+      break;
+    }
+    cudaEventElapsedTime(&ms0, ev[0], ev[1]);
+    cudaEventElapsedTime(&ms1, ev[1], ev[2]);
+    sum[0] += ms0;
+    sum[1] += ms1;
+  }
+  for (int i = 0; i < 3; ++i)
+    if (ev[i]) cudaEventDestroy(ev[i]);
+  if (rc != LEV_OK) return rc;
+  ms_out[0] = (float)(sum[0] / n);
+  ms_out[1] = (float)(sum[1] / n);
   return LEV_OK;
 }
 
@@ -1613,6 +1684,7 @@ int lev_autotune(LevEngine *h, float dt, int32_t trial_steps,
       float best_p = 0.0f;
       int best_pv = -1;
       for (int v = 0; v < kNumPairVariants && rc == LEV_OK; ++v) {
+        if (!pair_variant_ok(h, v)) continue;
         tc.pair_variant = v;
         for (int ph = 0; ph < 2 && rc == LEV_OK; ++ph) {  // warm-up
           a.reverse = ph;

@@ -12,12 +12,14 @@
 // Only the integrate of step t+1 needs a global value, g(t+1), which depends
 // on r(t+1) over all nodes.  So:
 //
-//   pair_kernel   step t complete (predictor, edges, integrate, r(t+1),
-//                 controller) and step t+1 without its integrate: the
+//   pair_kernel   step t complete (predictor, edges, integrate, tile
+//                 partials of r(t+1)) and step t+1 without its integrate: the
 //                 row's edges are walked twice back to back, the second
 //                 walk re-reading col/delay/weight from cache; S_i(t+1) and
 //                 eps_i(t+1) are parked in `pend`.
-//   finish_kernel the integrate of step t+1 with g(t+1), r(t+2), controller.
+//   reduce_kernel r(t+1) from the partials, controller -> g(t+1).
+//   finish_kernel the integrate of step t+1 with g(t+1), partials of r(t+2);
+//                 then reduce_kernel again.
 //
 // Each SELL entry (col/delay word, weight read and write) then leaves HBM
 // once per two steps, and the ring lines a tile gathers serve both steps
@@ -36,15 +38,12 @@
 
 namespace lev {
 
-// Block partial of (sum cos, sum sin) in the reference's tree order
-// (leviathan_kernel.cu:198-233), completion ticket and, in the last CTA of
-// the network, r (:242-263), the gain controller (:431-435) and the ring /
-// step-count advance.  The same sequence closes step_kernel.
-__device__ __forceinline__ void close_step(const StepArgs &a, const NetDesc &nd,
-                                           NetState *ns, int net, int row0,
-                                           float my_cos, float my_sin, float g,
-                                           int nxt, float *s_rc, float *s_rs,
-                                           int *s_last) {
+// Block partial of (sum cos, sum sin) of one 256-node tile in the
+// reference's tree order (leviathan_kernel.cu:198-233): warp shuffle trees,
+// then warp 0 over the eight warp sums.  All threads of the CTA call it.
+__device__ __forceinline__ void tile_partial(const StepArgs &a, const NetDesc &nd, int row0,
+                                             float my_cos, float my_sin, float *s_rc,
+                                             float *s_rs) {
   const int tid = threadIdx.x;
   const int lane = tid & 31, warp = tid >> 5;
   const unsigned mask = 0xffffffffu;
@@ -66,42 +65,64 @@ __device__ __forceinline__ void close_step(const StepArgs &a, const NetDesc &nd,
       my_cos += __shfl_down_sync(mask, my_cos, off);
       my_sin += __shfl_down_sync(mask, my_sin, off);
     }
-    if (lane == 0) {
-      a.partials[nd.part_off + row0 / kTile] = make_float2(my_cos, my_sin);
-      __threadfence();
-      const unsigned prev = atomicAdd(&ns->ticket, 1u);
-      *s_last = (prev == (unsigned)(nd.ntiles - 1));
-    }
+    if (lane == 0) a.partials[nd.part_off + row0 / kTile] = make_float2(my_cos, my_sin);
   }
-  __syncthreads();
-  if (!*s_last) return;
+}
 
-  __threadfence();
-  if (warp == 0) {
-    float sum_cos = 0.0f, sum_sin = 0.0f;
-    const float2 *part = a.partials + nd.part_off;
-    for (int k = lane; k < nd.ntiles; k += 32) {
-      const float2 v = __ldcg(part + k);
-      sum_cos += v.x;
-      sum_sin += v.y;
+constexpr int kReduceThreads = 1024;
+constexpr int kPartChunk = 4096;  // partials staged in shared memory per round
+
+// r and the gain controller of one network per CTA, after a pair_kernel or
+// finish_kernel launch has written every tile partial: the one-warp
+// lane-strided sums and shuffle tree of final_reduce_r_kernel
+// (leviathan_kernel.cu:242-263) -- lane l adds partials l, l+32, ... in turn
+// -- with the partials first staged in shared memory by the whole CTA, so
+// the sequential adds do not wait on L2; then the controller (:431-435) and
+// the ring / step-count advance.  nets: the networks of the launch's class.
+__global__ void __launch_bounds__(kReduceThreads) reduce_kernel(const StepArgs a,
+                                                                const int *nets) {
+  __shared__ float2 s_part[kPartChunk];
+  const int tid = threadIdx.x;
+  const int net = nets[blockIdx.x];
+  const NetDesc &nd = a.nets[net];
+  NetState *ns = a.st + net;
+  const int ntiles = nd.ntiles;
+  const float2 *part = a.partials + nd.part_off;
+  float sum_cos = 0.0f, sum_sin = 0.0f;
+  for (int c0 = 0; c0 < ntiles; c0 += kPartChunk) {
+    const int n = min(kPartChunk, ntiles - c0);
+    for (int k = tid; k < n; k += kReduceThreads) s_part[k] = part[c0 + k];
+    __syncthreads();
+    if (tid < 32) {
+#pragma unroll 8
+      for (int k = tid; k < n; k += 32) {
+        const float2 v = s_part[k];
+        sum_cos += v.x;
+        sum_sin += v.y;
+      }
     }
+    __syncthreads();
+  }
+  if (tid < 32) {
+    const unsigned mask = 0xffffffffu;
 #pragma unroll
     for (int off = 16; off > 0; off /= 2) {
       sum_cos += __shfl_down_sync(mask, sum_cos, off);
       sum_sin += __shfl_down_sync(mask, sum_sin, off);
     }
-    if (lane == 0) {
+    if (tid == 0) {
       float inv_N = 1.0f / (float)nd.N;
       float r = sqrtf(sum_cos * sum_cos + sum_sin * sum_sin) * inv_N;
+      const float g = ns->g;
       const float gn = nd.ctrl ? gain_controller(g, r, a.dt, nd) : g;
       ns->g = gn;
       ns->r = r;
-      ns->cur = nxt;
+      int nxt = ns->cur + 1;
+      ns->cur = (nxt == nd.bsi) ? 0 : nxt;
       int rb = ns->rbuf + 1;
       if (rb == nd.max_delay + 1) rb = 0;
       ns->rbuf = rb;
       ns->t = ns->t + 1;
-      ns->ticket = 0u;
       if (a.r_host) a.r_host[net] = r;
       if (a.r_hist) {
         const int k = ns->rpos;
@@ -112,11 +133,14 @@ __device__ __forceinline__ void close_step(const StepArgs &a, const NetDesc &nd,
   }
 }
 
+__device__ __forceinline__ int nxt_slot(int cur, int bsi) {
+  int nxt = cur + 1;
+  return nxt == bsi ? 0 : nxt;
+}
+
 // One step's walk over a lane's SELL row (csr_physics_kernel,
 // leviathan_kernel.cu:126-165): delayed phases from ring slot
 // (base - d) mod bsi, coupling sum in CSR order, Hebbian update in place.
-// Software-pipelined like step_kernel: the stream loads of group k0+U are in
-// flight while group k0 gathers and computes.
 //   SECOND = 0: first walk of the launch.  Stream loads stay cached (col /
 //               delay in L1 and L2, weights in L2) and the new weights are
 //               written to L2 for the second walk.
@@ -125,56 +149,51 @@ __device__ __forceinline__ void close_step(const StepArgs &a, const NetDesc &nd,
 //               loads).  Entries past the row's degree gather nothing: a
 //               padding entry (node 0, delay 0) would name the slot being
 //               written in this launch.
-template <int MATH, int U, int SECOND>
+//   DEEP = 0:   one-stage software pipeline (as step_kernel): the stream
+//               loads of group k0+U are in flight while group k0 gathers and
+//               computes.
+//   DEEP = 1:   two stages: while group k0 computes, the gathers of group
+//               k0+U (whose col/delay words arrived during the previous
+//               group) and the stream loads of group k0+2U are in flight.
+template <int MATH, int U, int SECOND, int DEEP>
 __device__ __forceinline__ float row_walk(const uint32_t *__restrict__ cdp,
-                                          float *__restrict__ wp, int len,
-                                          int deg, const float *__restrict__ ring,
-                                          int base, int bsi, int Np, float th,
-                                          float my_eps, float dt,
-                                          const NetDesc &nd) {
+                                          float *__restrict__ wp, int len, int deg,
+                                          const float *__restrict__ ring, int base,
+                                          int bsi, int Np, float th, float my_eps,
+                                          float dt, const NetDesc &nd) {
   const float eta = nd.eta, gamma = nd.gamma, lam = nd.lam;
   const float w_min = nd.w_min, w_max = nd.w_max;
   float local_sum = 0.0f;
-  uint32_t p[U];
-  float wv[U], dj[U];
+  auto load_streams = [&](int k0, uint32_t *p, float *w) {
 #pragma unroll
-  for (int u = 0; u < U; ++u) {
-    if (SECOND) {
-      p[u] = (u < len) ? __ldcs(cdp + 32 * u) : 0u;
-      wv[u] = (u < len) ? __ldcs(wp + 32 * u) : 0.0f;
-    } else {
-      p[u] = (u < len) ? __ldg(cdp + 32 * u) : 0u;
-      wv[u] = (u < len) ? __ldcg(wp + 32 * u) : 0.0f;
+    for (int u = 0; u < U; ++u) {
+      const int k = k0 + u;
+      if (SECOND) {
+        p[u] = (k < len) ? __ldcs(cdp + 32 * k) : 0u;
+        w[u] = (k < len) ? __ldcs(wp + 32 * k) : 0.0f;
+      } else {
+        p[u] = (k < len) ? __ldg(cdp + 32 * k) : 0u;
+        w[u] = (k < len) ? __ldcg(wp + 32 * k) : 0.0f;
+      }
     }
-  }
-  for (int k0 = 0; k0 < len; k0 += U) {
+  };
+  auto gather = [&](int k0, const uint32_t *p, float *g) {
 #pragma unroll
     for (int u = 0; u < U; ++u) {
       int slot = base - (int)(p[u] & 255u);
       slot += (slot < 0) ? bsi : 0;
       const float *src = ring + ((unsigned)slot * (unsigned)Np + (p[u] >> 8));
       if (SECOND)
-        dj[u] = (k0 + u < deg) ? ld_ring(src) : 0.0f;
+        g[u] = (k0 + u < deg) ? ld_ring(src) : 0.0f;
       else
-        dj[u] = ld_ring(src);
+        g[u] = ld_ring(src);
     }
-    uint32_t pn[U];
-    float wn[U];
-#pragma unroll
-    for (int u = 0; u < U; ++u) {
-      const int k = k0 + U + u;
-      if (SECOND) {
-        pn[u] = (k < len) ? __ldcs(cdp + 32 * k) : 0u;
-        wn[u] = (k < len) ? __ldcs(wp + 32 * k) : 0.0f;
-      } else {
-        pn[u] = (k < len) ? __ldg(cdp + 32 * k) : 0u;
-        wn[u] = (k < len) ? __ldcg(wp + 32 * k) : 0.0f;
-      }
-    }
+  };
+  auto compute = [&](int k0, const float *g, const float *wv) {
 #pragma unroll
     for (int u = 0; u < U; ++u) {
       if (k0 + u < deg) {
-        const float delayed_j = dj[u];
+        const float delayed_j = g[u];
         float diff = delayed_j - th;
         diff = wrap_pm_pi(diff);
         float w = wv[u];
@@ -191,21 +210,55 @@ __device__ __forceinline__ float row_walk(const uint32_t *__restrict__ cdp,
           __stcg(wp + 32 * (k0 + u), w);
       }
     }
+  };
+  if constexpr (DEEP) {
+    uint32_t pb[U];
+    float wa[U], wb[U], ga[U], gb[U];
+    {
+      uint32_t pa[U];
+      load_streams(0, pa, wa);
+      load_streams(U, pb, wb);
+      gather(0, pa, ga);
+    }
+    for (int k0 = 0; k0 < len; k0 += U) {
+      gather(k0 + U, pb, gb);
+      uint32_t pc[U];
+      float wc[U];
+      load_streams(k0 + 2 * U, pc, wc);
+      compute(k0, ga, wa);
 #pragma unroll
-    for (int u = 0; u < U; ++u) {
-      p[u] = pn[u];
-      wv[u] = wn[u];
+      for (int u = 0; u < U; ++u) {
+        ga[u] = gb[u];
+        wa[u] = wb[u];
+        pb[u] = pc[u];
+        wb[u] = wc[u];
+      }
+    }
+  } else {
+    uint32_t p[U];
+    float wv[U], dj[U];
+    load_streams(0, p, wv);
+    for (int k0 = 0; k0 < len; k0 += U) {
+      gather(k0, p, dj);
+      uint32_t pn[U];
+      float wn[U];
+      load_streams(k0 + U, pn, wn);
+      compute(k0, dj, wv);
+#pragma unroll
+      for (int u = 0; u < U; ++u) {
+        p[u] = pn[u];
+        wv[u] = wn[u];
+      }
     }
   }
   return local_sum;
 }
 
 // Step t in full and step t+1 up to its integrate (see the top of the file).
-template <int MATH, int U, int MINB>
+template <int MATH, int U, int MINB, int DEEP>
 __global__ void __launch_bounds__(kTile, MINB) pair_kernel(const StepArgs a) {
   __shared__ float s_rc[32];
   __shared__ float s_rs[32];
-  __shared__ int s_last;
 
   const int tid = threadIdx.x;
   const int lane = tid & 31, warp = tid >> 5;
@@ -223,6 +276,7 @@ __global__ void __launch_bounds__(kTile, MINB) pair_kernel(const StepArgs a) {
   const int bsi = nd.bsi;
   const int Np = nd.Np;
   const int cur = ns->cur;
+  const int nxt = nxt_slot(cur, bsi);
   const float g = ns->g;
   const float *ring = a.ring + nd.ring_off;
 
@@ -258,12 +312,10 @@ __global__ void __launch_bounds__(kTile, MINB) pair_kernel(const StepArgs a) {
   // ---- step t: edges (csr_physics_kernel, :126-165) -------------------------
   float sum0 = 0.0f;
   if (slice_live)
-    sum0 = row_walk<MATH, U, 0>(cdp, wp, len, deg, ring, cur, bsi, Np, th,
-                                fabsf(eps), dt, nd);
+    sum0 = row_walk<MATH, U, 0, DEEP>(cdp, wp, len, deg, ring, cur, bsi, Np, th, fabsf(eps),
+                                      dt, nd);
 
   // ---- step t: integrate (integrate_and_reduce_kernel, :182-196) ------------
-  int nxt = cur + 1;
-  if (nxt == bsi) nxt = 0;
   float my_cos = 0.0f, my_sin = 0.0f;
   float th1 = 0.0f, eps1 = 0.0f;
   if (live) {
@@ -286,53 +338,103 @@ __global__ void __launch_bounds__(kTile, MINB) pair_kernel(const StepArgs a) {
   // ---- step t+1: edges; the integrate waits for g(t+1) (finish_kernel) ------
   float sum1 = 0.0f;
   if (slice_live)
-    sum1 = row_walk<MATH, U, 1>(cdp, wp, len, deg, ring, nxt, bsi, Np, th1,
-                                fabsf(eps1), dt, nd);
+    sum1 = row_walk<MATH, U, 1, DEEP>(cdp, wp, len, deg, ring, nxt, bsi, Np, th1,
+                                      fabsf(eps1), dt, nd);
   if (live) a.pend[gi] = make_float2(sum1, eps1);
 
-  // ---- r(t+1), g(t+1) -------------------------------------------------------
-  close_step(a, nd, ns, tile.x, row0, my_cos, my_sin, g, nxt, s_rc, s_rs, &s_last);
+  // ---- partial of r(t+1); reduce_kernel forms r(t+1), g(t+1) ----------------
+  tile_partial(a, nd, row0, my_cos, my_sin, s_rc, s_rs);
 }
 
 // The integrate of step t+1 (integrate_and_reduce_kernel, :182-196) with
-// g(t+1), from the coupling sum and eps that pair_kernel parked; then
-// r(t+2) and the controller.
+// g(t+1), from the coupling sum and eps that pair_kernel parked, and the tile
+// partials of r(t+2).  A CTA takes kFinishTiles consecutive tiles of the
+// class's tile list (thread = one row of each), so the loads of all its rows
+// are in flight together and the launch is less than one wave deep.
+constexpr int kFinishTiles = 4;
+
 template <int MATH>
-__global__ void __launch_bounds__(kTile) finish_kernel(const StepArgs a) {
-  __shared__ float s_rc[32];
-  __shared__ float s_rs[32];
-  __shared__ int s_last;
+__global__ void __launch_bounds__(kTile) finish_kernel(const StepArgs a, int ntiles) {
+  __shared__ float s_rc[kFinishTiles][32];
+  __shared__ float s_rs[kFinishTiles][32];
 
   const int tid = threadIdx.x;
-  const int tix = a.reverse ? (int)(gridDim.x - 1 - blockIdx.x) : (int)blockIdx.x;
-  const int2 tile = a.tiles[tix];
-  const NetDesc nd = a.nets[tile.x];
-  NetState *ns = a.st + tile.x;
-
-  const int N = nd.N;
-  const int row0 = tile.y;
-  const int row = row0 + tid;
-  const long long gi = nd.node_off + row;
-  const float dt = a.dt;
-  const int cur = ns->cur;
-  const float g = ns->g;
-  int nxt = cur + 1;
-  if (nxt == nd.bsi) nxt = 0;
-
-  float my_cos = 0.0f, my_sin = 0.0f;
-  if (row < N) {
-    const float th = a.theta[gi];
-    const float2 pe = a.pend[gi];
-    const float local_sum = pe.x, eps = pe.y;
-    float inc = dt * (a.omega[gi] + g * local_sum - nd.alpha * eps);
-    float x = th + inc;
-    x = wrap_0_2pi(x);
-    if (!isfinite(x)) x = 0.0f;
-    a.theta[gi] = x;
-    a.ring[nd.ring_off + (long long)nxt * nd.Np + row] = x;
-    lev_sincos<MATH>(x, &my_sin, &my_cos);
+  const int lane = tid & 31, warp = tid >> 5;
+  float my_cos[kFinishTiles], my_sin[kFinishTiles];
+  float th[kFinishTiles], om[kFinishTiles];
+  float2 pe[kFinishTiles];
+  int2 tile[kFinishTiles];
+#pragma unroll
+  for (int q = 0; q < kFinishTiles; ++q) {
+    const int t = blockIdx.x * kFinishTiles + q;
+    tile[q] = make_int2(-1, 0);
+    if (t < ntiles) tile[q] = a.tiles[a.reverse ? ntiles - 1 - t : t];
   }
-  close_step(a, nd, ns, tile.x, row0, my_cos, my_sin, g, nxt, s_rc, s_rs, &s_last);
+#pragma unroll
+  for (int q = 0; q < kFinishTiles; ++q) {
+    my_cos[q] = my_sin[q] = 0.0f;
+    th[q] = om[q] = 0.0f;
+    pe[q] = make_float2(0.0f, 0.0f);
+    if (tile[q].x >= 0) {
+      const NetDesc &nd = a.nets[tile[q].x];
+      const int row = tile[q].y + tid;
+      if (row < nd.N) {
+        const long long gi = nd.node_off + row;
+        th[q] = a.theta[gi];
+        pe[q] = a.pend[gi];
+        om[q] = a.omega[gi];
+      }
+    }
+  }
+#pragma unroll
+  for (int q = 0; q < kFinishTiles; ++q) {
+    if (tile[q].x < 0) continue;
+    const NetDesc &nd = a.nets[tile[q].x];
+    const NetState *ns = a.st + tile[q].x;
+    const int row = tile[q].y + tid;
+    if (row < nd.N) {
+      const long long gi = nd.node_off + row;
+      const float g = ns->g;
+      int nxt = ns->cur + 1;
+      if (nxt == nd.bsi) nxt = 0;
+      const float local_sum = pe[q].x, eps = pe[q].y;
+      float inc = a.dt * (om[q] + g * local_sum - nd.alpha * eps);
+      float x = th[q] + inc;
+      x = wrap_0_2pi(x);
+      if (!isfinite(x)) x = 0.0f;
+      a.theta[gi] = x;
+      a.ring[nd.ring_off + (long long)nxt * nd.Np + row] = x;
+      lev_sincos<MATH>(x, &my_sin[q], &my_cos[q]);
+    }
+  }
+  // block partials in the tree order of tile_partial, warp q closing tile q
+  const unsigned mask = 0xffffffffu;
+#pragma unroll
+  for (int q = 0; q < kFinishTiles; ++q) {
+#pragma unroll
+    for (int off = 16; off > 0; off /= 2) {
+      my_cos[q] += __shfl_down_sync(mask, my_cos[q], off);
+      my_sin[q] += __shfl_down_sync(mask, my_sin[q], off);
+    }
+    if (lane == 0) {
+      s_rc[q][warp] = my_cos[q];
+      s_rs[q][warp] = my_sin[q];
+    }
+  }
+  __syncthreads();
+  if (warp < kFinishTiles && tile[warp].x >= 0) {
+    float c = (lane < (kTile / 32)) ? s_rc[warp][lane] : 0.0f;
+    float sn = (lane < (kTile / 32)) ? s_rs[warp][lane] : 0.0f;
+#pragma unroll
+    for (int off = 16; off > 0; off /= 2) {
+      c += __shfl_down_sync(mask, c, off);
+      sn += __shfl_down_sync(mask, sn, off);
+    }
+    if (lane == 0) {
+      const NetDesc &nd = a.nets[tile[warp].x];
+      a.partials[nd.part_off + tile[warp].y / kTile] = make_float2(c, sn);
+    }
+  }
 }
 
 }  // namespace lev

@@ -42,6 +42,14 @@ def variant_info(v: int) -> dict:
     return dict(unroll=u.value, pipelined=p.value, min_blocks=m.value)
 
 
+def pair_variant_info(v: int) -> dict:
+    """Tuning parameters of compiled two-steps-per-launch variant ``v``."""
+    lib = _lib.load()
+    u, m, dp = C.c_int32(), C.c_int32(), C.c_int32()
+    check(lib.lev_pair_variant_info(int(v), C.byref(u), C.byref(m), C.byref(dp)))
+    return dict(unroll=u.value, min_blocks=m.value, deep=dp.value)
+
+
 class _EngineBase:
     """Shared handle management and state access of both engine kinds."""
 
@@ -287,8 +295,8 @@ class _EngineBase:
     def pair_info(self) -> list:
         """Per degree class: whether two steps per launch are possible
         (eligible: no zero delay) and in use, the pair variant (-1: one step
-        per launch for this class) and the autotuner's ms per step of the
-        best pair and one-step variants (0 before autotuning)."""
+        per launch for this class), the autotuner's ms per step of the best
+        pair and one-step variants (0 before autotuning)."""
         out = []
         for c in range(3):
             el, en, pv = C.c_int32(), C.c_int32(), C.c_int32()
@@ -298,9 +306,7 @@ class _EngineBase:
             info = dict(cls=c, eligible=bool(el.value), enabled=bool(en.value),
                         pair_variant=pv.value, pair_ms=pms.value, step_ms=sms.value)
             if pv.value >= 0:
-                u, m = C.c_int32(), C.c_int32()
-                check(self._lib.lev_pair_variant_info(pv.value, C.byref(u), C.byref(m)))
-                info.update(unroll=u.value, min_blocks=m.value)
+                info.update(pair_variant_info(pv.value))
             out.append(info)
         return out
 
@@ -309,6 +315,14 @@ class _EngineBase:
 
     def set_pair_variant(self, cls: int, variant: int) -> None:
         check(self._lib.lev_set_pair_variant(self.handle, int(cls), int(variant)))
+
+    def time_launches(self, dt: float, n: int = 20) -> tuple:
+        """Mean durations (ms) of the two launch phases of a two-step round
+        (pair_kernel, finish_kernel -- or two one-step launches), timed with
+        CUDA events on the engine stream; advances the simulation 2n steps."""
+        ms = (C.c_float * 2)()
+        check(self._lib.lev_time_launches(self.handle, C.c_float(dt), int(n), ms))
+        return float(ms[0]), float(ms[1])
 
     # -- checkpoint ---------------------------------------------------------
     def get_state(self) -> dict:

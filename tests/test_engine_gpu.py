@@ -340,8 +340,10 @@ def test_two_steps_per_launch_bit_identical(mode):
     per launch: every pair variant, a single network at scale and a batch of
     uneven networks, odd block lengths, controller on and off."""
     from leviathan_v1_b200 import _lib
+    from leviathan_v1_b200.engine import pair_variant_info
 
     nvar = _lib.load().lev_num_pair_variants()
+    assert any(pair_variant_info(v)["deep"] for v in range(nvar))
     single = make_network(20_000, 16, 0.1, 30, seed=77)
     batch = [make_network(n, k, 0.1, md, seed=s)
              for n, k, md, s in [(700, 8, 10, 1), (2500, 20, 50, 2), (300, 4, 3, 3),
@@ -359,8 +361,7 @@ def test_two_steps_per_launch_bit_identical(mode):
         ref.close()
         for v in range(nvar):
             e = make()
-            if hasattr(e, "set_cluster_mode"):
-                e.set_cluster_mode(False)
+            e.set_cluster_mode(False)
             for c in range(3):
                 e.set_pair_variant(c, v)
             info = e.pair_info()
