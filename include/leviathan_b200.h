@@ -411,6 +411,48 @@ int lev_gen_ws(int32_t N, int32_t k, double p, uint64_t seed,
                float *theta, float *omega);
 
 /* ------------------------------------------------------------------------ */
+/* Hub-phase transition counts: the integrated-information front-end         */
+/* ------------------------------------------------------------------------ */
+
+/* The reference estimates a transition probability matrix of up to 10 "hub"
+ * nodes for its integrated-information solver: after every step the hub
+ * phases are binarised (bit i set when hub i's phase, taken modulo
+ * 6.2831853f into [0, 2pi), exceeds 3.1415926f) and the transition from the
+ * previous state is counted (binarize_and_accumulate_kernel,
+ * leviathan_phi_kernel.cu:60-92; in python/leviathan_iit_integration.py:
+ * 244-250 after a full host snapshot of all phases every step).  A LevHubs
+ * monitor counts the same transitions.  Attached to an engine it observes
+ * every step of one network inside the step's own reduction (no snapshot,
+ * no extra launch); standalone it observes a phase array in device memory,
+ * like phi_accumulate.  The integrated-information solver itself is not part
+ * of this library.
+ *
+ * lev_hubs_create    replaces phi_init (:243-287): num_hubs in [1, 10],
+ *                    hub_idx[num_hubs] node indices; S = 2^num_hubs states.
+ * lev_attach_hubs    every later step of network `net` of h is observed
+ *                    (m = NULL detaches).  While attached, the cluster-
+ *                    resident path is not used and lev_hubs_accumulate is
+ *                    refused.
+ * lev_hubs_accumulate replaces phi_accumulate (:289-298): one observation
+ *                    of theta_dev (device pointer; every hub index must be
+ *                    inside it) on `stream` (NULL: the monitor's own stream).
+ * lev_hubs_reset     replaces phi_reset (:337-345): counts 0, no previous
+ *                    state, no observations.
+ * lev_hubs_read      counts[S*S] (row = previous state), totals[S], the
+ *                    last state (-1 before any observation) and the number
+ *                    of observations (phi_get_transition_count, :347-349);
+ *                    each output may be NULL.  Waits for the feeding engine.
+ * lev_hubs_destroy   replaces phi_free (:351-367); detaches first. */
+typedef struct LevHubs LevHubs;
+int lev_hubs_create(LevHubs **out, int32_t num_hubs, const int32_t *hub_idx);
+int lev_attach_hubs(LevEngine *h, int32_t net, LevHubs *m);
+int lev_hubs_accumulate(LevHubs *m, const float *theta_dev, void *stream);
+int lev_hubs_reset(LevHubs *m);
+int lev_hubs_read(LevHubs *m, uint64_t *counts, uint64_t *totals, int32_t *prev_state,
+                  int64_t *observed);
+int lev_hubs_destroy(LevHubs *m);
+
+/* ------------------------------------------------------------------------ */
 /* Reference C ABI (leviathan_kernel.cu:21-499), same symbols and signatures */
 /* ------------------------------------------------------------------------ */
 typedef struct LeviathanHandle LeviathanHandle;

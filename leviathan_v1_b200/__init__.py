@@ -7,6 +7,8 @@ Public surface:
 * :class:`LeviathanObservatory` -- the reference's host API
   (python/leviathan_h100.py) on this engine;
 * :class:`BatchEngine` -- many independent networks per launch;
+* :class:`HubTransitions` -- hub-phase transition counts for the
+  integrated-information front-end, fed by the engine's own steps;
 * :mod:`.graphs` -- seeded topologies and initial states.
 
 The compute path is the CUDA library ``lib/libleviathan_b200.so`` (C ABI in
@@ -14,6 +16,7 @@ The compute path is the CUDA library ``lib/libleviathan_b200.so`` (C ABI in
 """
 
 from .engine import BatchEngine, LeviathanEngine  # noqa: F401
+from .hubs import HubTransitions  # noqa: F401
 from .observatory import LeviathanObservatory  # noqa: F401
 
-__all__ = ["LeviathanEngine", "LeviathanObservatory", "BatchEngine"]
+__all__ = ["LeviathanEngine", "LeviathanObservatory", "BatchEngine", "HubTransitions"]

@@ -131,6 +131,12 @@ PROTOTYPES = {
                                    _i32, _P]),
     "lev_gen_ws": (C.c_int, [_i32, _i32, C.c_double, C.c_uint64, _i32, _i32, _f32,
                              _f32, _f32, _f32, _P, _P, _P, _P, _P, _P]),
+    "lev_hubs_create": (C.c_int, [C.POINTER(_P), _i32, _P]),
+    "lev_attach_hubs": (C.c_int, [_P, _i32, _P]),
+    "lev_hubs_accumulate": (C.c_int, [_P, _P, _P]),
+    "lev_hubs_reset": (C.c_int, [_P]),
+    "lev_hubs_read": (C.c_int, [_P, _P, _P, C.POINTER(_i32), C.POINTER(_i64)]),
+    "lev_hubs_destroy": (C.c_int, [_P]),
     # reference ABI (leviathan_kernel.cu:21-499)
     "leviathan_init": (_P, [C.c_int, C.c_int, _P, _P, _P, _P, _P, _P, _P]),
     "leviathan_step": (_f32, [_P, _f32]),

@@ -131,6 +131,8 @@ inline std::tuple<int, int, int> tune_key(const TileClass &tc, int c) {
 
 using namespace lev;
 
+struct LevHubs;
+
 struct LevEngine {
   int device = 0;
   cudaStream_t stream = nullptr;
@@ -169,6 +171,7 @@ struct LevEngine {
   bool use_pairs = true;
   float2 *d_pend = nullptr;  // [total_nodes] parked (coupling sum, eps)
   int *d_class_nets = nullptr;  // networks of each class, class by class
+  LevHubs *hubs = nullptr;      // attached hub monitor (lev_attach_hubs)
 
   // r of the last single step, written by the kernel into mapped host memory
   float *h_rmap = nullptr;
@@ -195,6 +198,18 @@ struct LeviathanHandle {
   LevEngine *eng;
 };
 
+// Hub-phase transition counter (HubMonitor on the device).
+struct LevHubs {
+  int device = 0;
+  int num_hubs = 0;
+  int S = 0;  // 2^num_hubs states
+  HubMonitor *d_mon = nullptr;
+  unsigned long long *d_counts = nullptr;  // [S][S]
+  unsigned long long *d_totals = nullptr;  // [S]
+  cudaStream_t stream = nullptr;           // standalone observations
+  LevEngine *engine = nullptr;             // engine that feeds it, if attached
+};
+
 namespace {
 
 template <typename T>
@@ -213,6 +228,7 @@ int dev_alloc(LevEngine *h, T **p, size_t count) {
 
 void free_engine(LevEngine *h) {
   if (!h) return;
+  if (h->hubs) h->hubs->engine = nullptr;
   for (auto &kv : h->graphs) {
     if (kv.second.exec) cudaGraphExecDestroy(kv.second.exec);
     if (kv.second.graph) cudaGraphDestroy(kv.second.graph);
@@ -322,6 +338,7 @@ StepArgs make_args(LevEngine *h, float dt, float *r_hist, int r_cap,
   a.dt = dt;
   a.reverse = 0;
   a.pend = h->d_pend;
+  a.hubs = h->hubs ? h->hubs->d_mon : nullptr;
   return a;
 }
 
@@ -590,7 +607,7 @@ int enqueue_steps(LevEngine *h, float dt, int n, float *stage) {
   int done = 0;
   while (done < n) {
     const int len = std::min(h->block_len, n - done);
-    if (h->cluster_ok && h->use_cluster) {
+    if (h->cluster_ok && h->use_cluster && !h->hubs) {
       int rc = launch_cluster(h, dt, len);
       if (rc != LEV_OK) return rc;
     } else {
@@ -1680,7 +1697,7 @@ int lev_autotune(LevEngine *h, float dt, int32_t trial_steps,
     // two steps per launch: pair_kernel + finish_kernel per two steps; kept
     // for this class only where it beats the best one-step variant
     if (h->pair_ok && rc == LEV_OK) {
-      const int pairs = std::max(1, trial_steps / 2);
+      const int pairs = std::max(1, trial_steps);
       float best_p = 0.0f;
       int best_pv = -1;
       for (int v = 0; v < kNumPairVariants && rc == LEV_OK; ++v) {
@@ -1747,6 +1764,161 @@ int lev_get_vram_usage(const LevEngine *h, size_t *bytes) {
   *bytes = h->vram;
   return LEV_OK;
 }
+
+// ===========================================================================
+// Hub-phase transition counter (the reference's integrated-information
+// front-end, leviathan_phi_kernel.cu:60-92 and phi_init / phi_accumulate /
+// phi_reset / phi_get_transition_count / phi_free, :243-367)
+// ===========================================================================
+namespace lev {
+__global__ void hub_observe_kernel(HubMonitor *m, const float *theta) {
+  if (threadIdx.x == 0 && blockIdx.x == 0) hub_observe(m, theta);
+}
+}  // namespace lev
+
+static int hubs_sync(LevHubs *m) {
+  if (m->engine) LEV_TRY_CUDA(cudaStreamSynchronize(m->engine->stream));
+  LEV_TRY_CUDA(cudaStreamSynchronize(m->stream));
+  return LEV_OK;
+}
+
+static int hubs_clear(LevHubs *m) {
+  const size_t S = (size_t)m->S;
+  LEV_TRY_CUDA(cudaMemsetAsync(m->d_counts, 0, sizeof(unsigned long long) * S * S, m->stream));
+  LEV_TRY_CUDA(cudaMemsetAsync(m->d_totals, 0, sizeof(unsigned long long) * S, m->stream));
+  const int prev = -1;
+  const long long observed = 0;
+  LEV_TRY_CUDA(cudaMemcpyAsync(&m->d_mon->prev, &prev, sizeof(int), cudaMemcpyHostToDevice,
+                               m->stream));
+  LEV_TRY_CUDA(cudaMemcpyAsync(&m->d_mon->observed, &observed, sizeof(long long),
+                               cudaMemcpyHostToDevice, m->stream));
+  LEV_TRY_CUDA(cudaStreamSynchronize(m->stream));
+  return LEV_OK;
+}
+
+static void hubs_free(LevHubs *m) {
+  cudaFree(m->d_mon);
+  cudaFree(m->d_counts);
+  cudaFree(m->d_totals);
+  if (m->stream) cudaStreamDestroy(m->stream);
+  delete m;
+}
+
+extern "C" {
+
+int lev_hubs_create(LevHubs **out, int32_t num_hubs, const int32_t *hub_idx) {
+  if (!out || !hub_idx) return fail(LEV_ERR_ARG, "null argument");
+  *out = nullptr;
+  if (num_hubs < 1 || num_hubs > kMaxHubs)
+    return fail(LEV_ERR_ARG, "num_hubs must be in [1, " + std::to_string(kMaxHubs) + "]");
+  for (int i = 0; i < num_hubs; ++i)
+    if (hub_idx[i] < 0) return fail(LEV_ERR_ARG, "hub index is negative");
+  LevHubs *m = new LevHubs();
+  m->num_hubs = num_hubs;
+  m->S = 1 << num_hubs;
+  cudaError_t e = cudaGetDevice(&m->device);
+  if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&m->stream, cudaStreamNonBlocking);
+  if (e == cudaSuccess) e = cudaMalloc(&m->d_mon, sizeof(HubMonitor));
+  if (e == cudaSuccess)
+    e = cudaMalloc(&m->d_counts, sizeof(unsigned long long) * (size_t)m->S * m->S);
+  if (e == cudaSuccess) e = cudaMalloc(&m->d_totals, sizeof(unsigned long long) * m->S);
+  if (e != cudaSuccess) {
+    hubs_free(m);
+    return fail(LEV_ERR_NOMEM, std::string("hub monitor: ") + cudaGetErrorString(e));
+  }
+  HubMonitor hm;
+  std::memset(&hm, 0, sizeof(hm));
+  hm.net = -1;
+  hm.num_hubs = num_hubs;
+  for (int i = 0; i < num_hubs; ++i) hm.hub[i] = hub_idx[i];
+  hm.prev = -1;
+  hm.counts = m->d_counts;
+  hm.totals = m->d_totals;
+  e = cudaMemcpy(m->d_mon, &hm, sizeof(hm), cudaMemcpyHostToDevice);
+  int rc = e == cudaSuccess ? hubs_clear(m)
+                            : fail(LEV_ERR_CUDA, std::string("hub monitor: ") + cudaGetErrorString(e));
+  if (rc != LEV_OK) {
+    std::string msg = g_last_error;
+    hubs_free(m);
+    return fail(rc, msg);
+  }
+  *out = m;
+  return LEV_OK;
+}
+
+int lev_attach_hubs(LevEngine *h, int32_t net, LevHubs *m) {
+  if (!h) return fail(LEV_ERR_ARG, "null handle");
+  DeviceScope ds(h->device);
+  LEV_TRY_CUDA(cudaStreamSynchronize(h->stream));
+  if (!m) {  // detach
+    if (h->hubs) {
+      h->hubs->engine = nullptr;
+      h->hubs = nullptr;
+      clear_graphs(h);
+    }
+    return LEV_OK;
+  }
+  if (net < 0 || net >= h->num_nets) return fail(LEV_ERR_ARG, "network out of range");
+  if (m->device != h->device) return fail(LEV_ERR_ARG, "hub monitor is on another device");
+  if (m->engine && m->engine != h) return fail(LEV_ERR_STATE, "hub monitor fed by another engine");
+  HubMonitor hm;
+  LEV_TRY_CUDA(cudaMemcpy(&hm, m->d_mon, sizeof(hm), cudaMemcpyDeviceToHost));
+  for (int i = 0; i < m->num_hubs; ++i)
+    if (hm.hub[i] >= h->h_nets[net].N) return fail(LEV_ERR_ARG, "hub index beyond the network");
+  if (h->hubs && h->hubs != m) h->hubs->engine = nullptr;
+  hm.net = net;
+  LEV_TRY_CUDA(cudaMemcpy(&m->d_mon->net, &hm.net, sizeof(int), cudaMemcpyHostToDevice));
+  h->hubs = m;
+  m->engine = h;
+  clear_graphs(h);
+  return LEV_OK;
+}
+
+int lev_hubs_accumulate(LevHubs *m, const float *theta_dev, void *stream) {
+  if (!m || !theta_dev) return fail(LEV_ERR_ARG, "null argument");
+  if (m->engine) return fail(LEV_ERR_STATE, "hub monitor is fed by an engine; detach it first");
+  DeviceScope ds(m->device);
+  cudaStream_t s = stream ? reinterpret_cast<cudaStream_t>(stream) : m->stream;
+  hub_observe_kernel<<<1, 32, 0, s>>>(m->d_mon, theta_dev);
+  LEV_TRY_CUDA(cudaGetLastError());
+  if (s != m->stream) LEV_TRY_CUDA(cudaStreamSynchronize(s));
+  return LEV_OK;
+}
+
+int lev_hubs_reset(LevHubs *m) {
+  if (!m) return fail(LEV_ERR_ARG, "null argument");
+  DeviceScope ds(m->device);
+  int rc = hubs_sync(m);
+  return rc != LEV_OK ? rc : hubs_clear(m);
+}
+
+int lev_hubs_read(LevHubs *m, uint64_t *counts, uint64_t *totals, int32_t *prev_state,
+                  int64_t *observed) {
+  if (!m) return fail(LEV_ERR_ARG, "null argument");
+  DeviceScope ds(m->device);
+  int rc = hubs_sync(m);
+  if (rc != LEV_OK) return rc;
+  const size_t S = (size_t)m->S;
+  if (counts)
+    LEV_TRY_CUDA(cudaMemcpy(counts, m->d_counts, sizeof(uint64_t) * S * S, cudaMemcpyDeviceToHost));
+  if (totals)
+    LEV_TRY_CUDA(cudaMemcpy(totals, m->d_totals, sizeof(uint64_t) * S, cudaMemcpyDeviceToHost));
+  HubMonitor hm;
+  LEV_TRY_CUDA(cudaMemcpy(&hm, m->d_mon, sizeof(hm), cudaMemcpyDeviceToHost));
+  if (prev_state) *prev_state = hm.prev;
+  if (observed) *observed = hm.observed;
+  return LEV_OK;
+}
+
+int lev_hubs_destroy(LevHubs *m) {
+  if (!m) return LEV_OK;
+  DeviceScope ds(m->device);
+  if (m->engine) lev_attach_hubs(m->engine, 0, nullptr);
+  hubs_free(m);
+  return LEV_OK;
+}
+
+}  // extern "C"
 
 // ===========================================================================
 // Reference ABI (leviathan_kernel.cu:21-499)

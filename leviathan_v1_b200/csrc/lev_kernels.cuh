@@ -86,6 +86,45 @@ struct NetState {
   int rpos;         // next row of the r history
 };
 
+// Hub-phase transition counter: the front-end of the reference's integrated-
+// information solver (binarize_and_accumulate_kernel,
+// leviathan_phi_kernel.cu:60-92), fed by the engine after every step of one
+// network instead of by a host snapshot of all phases.
+constexpr int kMaxHubs = 10;  // the reference solver's limit (1024 states)
+struct HubMonitor {
+  int net;                     // watched network (-1: standalone)
+  int num_hubs;                // 1 .. kMaxHubs
+  int hub[kMaxHubs];           // hub node indices, local to the network
+  int prev;                    // state after the previous observation, -1 before the first
+  int pad;
+  long long observed;          // observations (accumulate calls)
+  unsigned long long *counts;  // [S][S] transitions prev -> state, S = 2^num_hubs
+  unsigned long long *totals;  // [S] transitions out of each state
+};
+
+// One observation (binarize_and_accumulate_kernel, leviathan_phi_kernel.cu:
+// 67-91): bit i of the state is set when hub i's phase, taken modulo
+// 6.2831853f into [0, 2pi), exceeds 3.1415926f; the transition from the
+// previous state is counted.  One thread; theta read through L2 because
+// other CTAs of the same launch may have written it.
+__device__ __forceinline__ void hub_observe(HubMonitor *hm, const float *theta) {
+  int state = 0;
+  for (int i = 0; i < hm->num_hubs; ++i) {
+    float phase = __ldcg(theta + hm->hub[i]);
+    phase = fmodf(phase, 6.2831853f);
+    if (phase < 0) phase += 6.2831853f;
+    if (phase > 3.1415926f) state |= (1 << i);
+  }
+  const int S = 1 << hm->num_hubs;
+  const int prev = hm->prev;
+  if (prev >= 0 && prev < S) {
+    hm->counts[(long long)prev * S + state] += 1ull;
+    hm->totals[prev] += 1ull;
+  }
+  hm->prev = state;
+  hm->observed += 1;
+}
+
 struct StepArgs {
   const NetDesc *nets;
   NetState *st;
@@ -108,6 +147,7 @@ struct StepArgs {
   float dt;
   int reverse;  // 1: CTAs walk the tile list backwards (alternating sweeps)
   float2 *pend;  // [nodes] (coupling sum, eps) of a half-done step (lev_pair.cuh)
+  HubMonitor *hubs;  // observes hub phases after every step of hubs->net, or null
 };
 
 // ---------------------------------------------------------------------------
@@ -397,6 +437,7 @@ __global__ void __launch_bounds__(kTile, MINB) step_kernel(const StepArgs a) {
         if (k < a.r_cap) a.r_hist[(long long)k * a.num_nets + tile.x] = r;
         ns->rpos = k + 1;
       }
+      if (a.hubs && a.hubs->net == tile.x) hub_observe(a.hubs, a.theta + nd.node_off);
     }
   }
 }

@@ -84,8 +84,11 @@ __global__ void __launch_bounds__(kReduceThreads) reduce_kernel(const StepArgs a
   __shared__ float2 s_part[kPartChunk];
   const int tid = threadIdx.x;
   const int net = nets[blockIdx.x];
-  const NetDesc &nd = a.nets[net];
+  const NetDesc nd = a.nets[net];
   NetState *ns = a.st + net;
+  // network state read up front, off the partial-sum critical path
+  NetState st;
+  if (tid == 0) st = *ns;
   const int ntiles = nd.ntiles;
   const float2 *part = a.partials + nd.part_off;
   float sum_cos = 0.0f, sum_sin = 0.0f;
@@ -113,22 +116,21 @@ __global__ void __launch_bounds__(kReduceThreads) reduce_kernel(const StepArgs a
     if (tid == 0) {
       float inv_N = 1.0f / (float)nd.N;
       float r = sqrtf(sum_cos * sum_cos + sum_sin * sum_sin) * inv_N;
-      const float g = ns->g;
-      const float gn = nd.ctrl ? gain_controller(g, r, a.dt, nd) : g;
-      ns->g = gn;
-      ns->r = r;
-      int nxt = ns->cur + 1;
-      ns->cur = (nxt == nd.bsi) ? 0 : nxt;
-      int rb = ns->rbuf + 1;
-      if (rb == nd.max_delay + 1) rb = 0;
-      ns->rbuf = rb;
-      ns->t = ns->t + 1;
+      const float g = st.g;
+      st.g = nd.ctrl ? gain_controller(g, r, a.dt, nd) : g;
+      st.r = r;
+      const int nxt = st.cur + 1;
+      st.cur = (nxt == nd.bsi) ? 0 : nxt;
+      const int rb = st.rbuf + 1;
+      st.rbuf = (rb == nd.max_delay + 1) ? 0 : rb;
+      st.t = st.t + 1;
       if (a.r_host) a.r_host[net] = r;
       if (a.r_hist) {
-        const int k = ns->rpos;
-        if (k < a.r_cap) a.r_hist[(long long)k * a.num_nets + net] = r;
-        ns->rpos = k + 1;
+        if (st.rpos < a.r_cap) a.r_hist[(long long)st.rpos * a.num_nets + net] = r;
+        st.rpos = st.rpos + 1;
       }
+      *ns = st;
+      if (a.hubs && a.hubs->net == net) hub_observe(a.hubs, a.theta + nd.node_off);
     }
   }
 }
