@@ -2178,6 +2178,14 @@ struct LevAdjoint {
         *ck_w = nullptr, *ck_ring = nullptr, *ck_g = nullptr;
   float *w_hist = nullptr, *thh_hist = nullptr;
   float4 *trace = nullptr;
+  // second set of segment records (extended ring, weights, theta_hat, trace)
+  // so the backward pass recomputes segment k-1 on `rstream` while segment k
+  // is reversed on the engine stream; null when it did not fit
+  float *ring2 = nullptr, *w_hist2 = nullptr, *thh_hist2 = nullptr;
+  float4 *trace2 = nullptr;
+  cudaStream_t rstream = nullptr;
+  cudaEvent_t ev_rec[2] = {nullptr, nullptr}, ev_rev[2] = {nullptr, nullptr},
+              ev_start = nullptr;
   float *lam_th = nullptr, *lam_thh = nullptr, *lam_omh = nullptr,
         *lam_w = nullptr, *adj_ring = nullptr, *lam_g = nullptr,
         *grad_omega_acc = nullptr, *grad_theta0 = nullptr;
@@ -2214,6 +2222,12 @@ int adj_alloc(LevAdjoint *a, T **p, long long count) {
 void adj_free(LevAdjoint *a) {
   if (!a) return;
   for (void *p : a->allocs) cudaFree(p);
+  for (int i = 0; i < 2; ++i) {
+    if (a->ev_rec[i]) cudaEventDestroy(a->ev_rec[i]);
+    if (a->ev_rev[i]) cudaEventDestroy(a->ev_rev[i]);
+  }
+  if (a->ev_start) cudaEventDestroy(a->ev_start);
+  if (a->rstream) cudaStreamDestroy(a->rstream);
   delete a;
 }
 
@@ -2240,19 +2254,24 @@ AdjFwdArgs adj_fwd_args(LevAdjoint *a, float dt) {
   return f;
 }
 
-int adj_launch_fwd(LevAdjoint *a, const AdjFwdArgs &f) {
+int adj_launch_fwd(LevAdjoint *a, const AdjFwdArgs &f, cudaStream_t s = nullptr) {
   LevEngine *e = a->e;
+  if (!s) s = e->stream;
   if (e->math_mode == LEV_MATH_ACCURATE)
-    adj_fwd_kernel<1><<<e->total_tiles, kTile, 0, e->stream>>>(f);
+    adj_fwd_kernel<1><<<e->total_tiles, kTile, 0, s>>>(f);
   else
-    adj_fwd_kernel<0><<<e->total_tiles, kTile, 0, e->stream>>>(f);
+    adj_fwd_kernel<0><<<e->total_tiles, kTile, 0, s>>>(f);
   LEV_TRY_CUDA(cudaGetLastError());
   return LEV_OK;
 }
 
-int adj_ckpt(LevAdjoint *a, int seg, bool save) {
+// Checkpoint `seg` of the working state: save (forward pass) or restore into
+// the working state and the extended ring `ring` (backward recompute).
+int adj_ckpt(LevAdjoint *a, int seg, bool save, cudaStream_t s = nullptr,
+             float *ring = nullptr) {
   LevEngine *e = a->e;
-  cudaStream_t s = e->stream;
+  if (!s) s = e->stream;
+  if (!ring) ring = a->ring;
   const size_t nb = sizeof(float) * a->TN;
   auto cp = [&](float *ck, float *live, size_t bytes) {
     return save ? cudaMemcpyAsync(ck, live, bytes, cudaMemcpyDeviceToDevice, s)
@@ -2267,11 +2286,11 @@ int adj_ckpt(LevAdjoint *a, int seg, bool save) {
   if (save) {
     adj_state_kernel<<<1, 128, 0, s>>>(1, a->d_nets, a->d_st,
                                        a->ck_g + (size_t)seg * a->NN, nullptr, a->NN);
-    adj_ring_ckpt_kernel<<<grid, 256, 0, s>>>(0, a->d_nets, a->d_st, a->ring,
+    adj_ring_ckpt_kernel<<<grid, 256, 0, s>>>(0, a->d_nets, a->d_st, ring,
                                               a->ck_ring + (size_t)seg * a->ckr_floats,
                                               a->d_ck_off, a->NN);
   } else {
-    adj_ring_ckpt_kernel<<<grid, 256, 0, s>>>(1, a->d_nets, a->d_st, a->ring,
+    adj_ring_ckpt_kernel<<<grid, 256, 0, s>>>(1, a->d_nets, a->d_st, ring,
                                               a->ck_ring + (size_t)seg * a->ckr_floats,
                                               a->d_ck_off, a->NN);
     adj_state_kernel<<<1, 128, 0, s>>>(2, a->d_nets, a->d_st,
@@ -2345,6 +2364,27 @@ int lev_adj_create(LevAdjoint **out, LevEngine *e, int32_t segment,
   A(a->lam_g, NN);
   A(a->grad_omega_acc, TN);
   A(a->grad_theta0, TN);
+  if (rc == LEV_OK && S > 1) {
+    // optional second record set; without it the backward pass runs the
+    // recompute and the reverse steps of each segment one after the other
+    size_t fr = 0, tot = 0;
+    const size_t need = sizeof(float) * ((size_t)a->ring_floats + (size_t)(C + 1) * SL +
+                                         (size_t)C * TN) + sizeof(float4) * (size_t)C * NN;
+    if (cudaMemGetInfo(&fr, &tot) == cudaSuccess && need + (256ull << 20) < fr) {
+      A(a->ring2, a->ring_floats);
+      A(a->w_hist2, (C + 1) * SL);
+      A(a->thh_hist2, C * TN);
+      A(a->trace2, C * NN);
+      if (rc == LEV_OK &&
+          (cudaStreamCreateWithFlags(&a->rstream, cudaStreamNonBlocking) != cudaSuccess ||
+           cudaEventCreateWithFlags(&a->ev_rec[0], cudaEventDisableTiming) != cudaSuccess ||
+           cudaEventCreateWithFlags(&a->ev_rec[1], cudaEventDisableTiming) != cudaSuccess ||
+           cudaEventCreateWithFlags(&a->ev_rev[0], cudaEventDisableTiming) != cudaSuccess ||
+           cudaEventCreateWithFlags(&a->ev_rev[1], cudaEventDisableTiming) != cudaSuccess ||
+           cudaEventCreateWithFlags(&a->ev_start, cudaEventDisableTiming) != cudaSuccess))
+        rc = fail(LEV_ERR_CUDA, "adjoint: stream or event creation failed");
+    }
+  }
 #undef A
   if (rc != LEV_OK) {
     std::string msg = g_last_error;
@@ -2476,19 +2516,33 @@ int lev_adj_backward(LevAdjoint *a, const float *dLdr, const float *dLdtheta,
   if (a->res_grb) LEV_TRY_CUDA(cudaMemsetAsync(a->res_grb, 0, nb, s));
   const int nseg = (T + a->C - 1) / a->C;
   const int mode = (e->math_mode == LEV_MATH_ACCURATE) ? 1 : 0;
-  for (int seg = nseg - 1; seg >= 0; --seg) {
+  // Segment k-1 is recomputed (stream rs, record set (k-1)&1) while segment k
+  // is reversed (engine stream, record set k&1), when the second set exists.
+  const bool overlap = a->rstream != nullptr && nseg > 1;
+  float *rings[2] = {a->ring, overlap ? a->ring2 : a->ring};
+  float *whs[2] = {a->w_hist, overlap ? a->w_hist2 : a->w_hist};
+  float *ths[2] = {a->thh_hist, overlap ? a->thh_hist2 : a->thh_hist};
+  float4 *trs[2] = {a->trace, overlap ? a->trace2 : a->trace};
+  cudaStream_t rs = overlap ? a->rstream : s;
+  if (overlap) {
+    LEV_TRY_CUDA(cudaEventRecord(a->ev_start, s));
+    LEV_TRY_CUDA(cudaStreamWaitEvent(rs, a->ev_start, 0));
+  }
+  // recompute a segment forward, recording what its reverse steps need
+  auto recompute = [&](int seg) -> int {
+    const int buf = seg & 1;
     const int s0 = seg * a->C, s1 = std::min(T, s0 + a->C);
-    // recompute the segment forward, recording what the reverse steps need
-    int rc = adj_ckpt(a, seg, false);
+    int rc = adj_ckpt(a, seg, false, rs, rings[buf]);
     if (rc != LEV_OK) return rc;
-    LEV_TRY_CUDA(cudaMemcpyAsync(a->w_hist, a->w, wb, cudaMemcpyDeviceToDevice, s));
+    LEV_TRY_CUDA(cudaMemcpyAsync(whs[buf], a->w, wb, cudaMemcpyDeviceToDevice, rs));
     AdjFwdArgs f = adj_fwd_args(a, dt);
+    f.ring = rings[buf];
     for (int t = s0; t < s1; ++t) {
       const int k = t - s0;
-      f.w_in = a->w_hist + (size_t)k * a->SL;
-      f.w_out = a->w_hist + (size_t)(k + 1) * a->SL;
-      f.thh_rec = a->thh_hist + (size_t)k * a->TN;
-      f.trace = a->trace + (size_t)k * a->NN;
+      f.w_in = whs[buf] + (size_t)k * a->SL;
+      f.w_out = whs[buf] + (size_t)(k + 1) * a->SL;
+      f.thh_rec = ths[buf] + (size_t)k * a->TN;
+      f.trace = trs[buf] + (size_t)k * a->NN;
       f.drive = a->drive ? a->drive + (size_t)t * a->TN : nullptr;
       f.r_out = nullptr;
       f.theta_out = nullptr;
@@ -2496,9 +2550,19 @@ int lev_adj_backward(LevAdjoint *a, const float *dLdr, const float *dLdtheta,
         f.win = a->res_win;
         f.xin = a->res_x + (size_t)t * a->NN;
       }
-      rc = adj_launch_fwd(a, f);
+      rc = adj_launch_fwd(a, f, rs);
       if (rc != LEV_OK) return rc;
     }
+    if (overlap) LEV_TRY_CUDA(cudaEventRecord(a->ev_rec[buf], rs));
+    return LEV_OK;
+  };
+  bool rev_recorded[2] = {false, false};
+  int rc = recompute(nseg - 1);
+  if (rc != LEV_OK) return rc;
+  for (int seg = nseg - 1; seg >= 0; --seg) {
+    const int buf = seg & 1;
+    const int s0 = seg * a->C, s1 = std::min(T, s0 + a->C);
+    if (overlap) LEV_TRY_CUDA(cudaStreamWaitEvent(s, a->ev_rec[buf], 0));
     // reverse steps
     AdjBwdArgs b;
     std::memset(&b, 0, sizeof(b));
@@ -2508,7 +2572,7 @@ int lev_adj_backward(LevAdjoint *a, const float *dLdr, const float *dLdtheta,
     b.sl_off = e->d_sl_off;
     b.sl_len = e->d_sl_len;
     b.sl_cd = e->d_sl_cd;
-    b.H = a->ring;
+    b.H = rings[buf];
     b.lam_th = a->lam_th;
     b.lam_thh = a->lam_thh;
     b.lam_omh = a->lam_omh;
@@ -2523,9 +2587,9 @@ int lev_adj_backward(LevAdjoint *a, const float *dLdr, const float *dLdtheta,
     for (int t = s1 - 1; t >= s0; --t) {
       const int k = t - s0;
       b.s = t;
-      b.w_s = a->w_hist + (size_t)k * a->SL;
-      b.thh_s = a->thh_hist + (size_t)k * a->TN;
-      b.trace = a->trace + (size_t)k * a->NN;
+      b.w_s = whs[buf] + (size_t)k * a->SL;
+      b.thh_s = ths[buf] + (size_t)k * a->TN;
+      b.trace = trs[buf] + (size_t)k * a->NN;
       b.dLdr = dLdr ? dLdr + (size_t)t * a->NN : nullptr;
       b.dLdth = dLdtheta ? dLdtheta + (size_t)t * a->TN : nullptr;
       b.grad_drive = grad_drive ? grad_drive + (size_t)t * a->TN : nullptr;
@@ -2546,6 +2610,18 @@ int lev_adj_backward(LevAdjoint *a, const float *dLdr, const float *dLdtheta,
       else
         adj_bwd_kernel<0><<<e->total_tiles, kTile, 0, s>>>(b);
       LEV_TRY_CUDA(cudaGetLastError());
+    }
+    if (overlap) {
+      LEV_TRY_CUDA(cudaEventRecord(a->ev_rev[buf], s));
+      rev_recorded[buf] = true;
+    }
+    if (seg > 0) {
+      // the record set of segment seg-1 was last read by the reverse of seg+1
+      const int nbuf = (seg - 1) & 1;
+      if (overlap && rev_recorded[nbuf])
+        LEV_TRY_CUDA(cudaStreamWaitEvent(rs, a->ev_rev[nbuf], 0));
+      rc = recompute(seg - 1);
+      if (rc != LEV_OK) return rc;
     }
   }
   // gradients
