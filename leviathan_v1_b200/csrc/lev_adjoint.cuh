@@ -113,21 +113,32 @@ __global__ void __launch_bounds__(kTile, 3) adj_fwd_kernel(const AdjFwdArgs a) {
     const long long s = nd.slice_base + (slice_row0 >> 5);
     const int len = a.sl_len[s];
     const long long base = a.sl_off[s] + lane;
+    // software-pipelined like step_kernel: the stream loads of group k0+U
+    // are in flight while group k0 gathers and computes
     constexpr int U = 8;
-    for (int k0 = 0; k0 < len; k0 += U) {
-      uint32_t p[U];
-      float wv[U], dj[U];
+    uint32_t p[U];
+    float wv[U];
 #pragma unroll
-      for (int u = 0; u < U; ++u) {
-        const bool in = k0 + u < len;
-        p[u] = in ? __ldg(a.sl_cd + base + 32 * (k0 + u)) : 0u;
-        wv[u] = in ? a.w_in[base + 32 * (k0 + u)] : 0.0f;
-      }
+    for (int u = 0; u < U; ++u) {
+      const bool in = u < len;
+      p[u] = in ? __ldg(a.sl_cd + base + 32 * u) : 0u;
+      wv[u] = in ? a.w_in[base + 32 * u] : 0.0f;
+    }
+    for (int k0 = 0; k0 < len; k0 += U) {
+      float dj[U];
 #pragma unroll
       for (int u = 0; u < U; ++u) {
         int slot = cur - (int)(p[u] & 255u);
         slot += (slot < 0) ? bsi : 0;
         dj[u] = ld_ring(ring + ((unsigned)slot * (unsigned)Np + (p[u] >> 8)));
+      }
+      uint32_t pn[U];
+      float wn[U];
+#pragma unroll
+      for (int u = 0; u < U; ++u) {
+        const bool in = k0 + U + u < len;
+        pn[u] = in ? __ldg(a.sl_cd + base + 32 * (k0 + U + u)) : 0u;
+        wn[u] = in ? a.w_in[base + 32 * (k0 + U + u)] : 0.0f;
       }
 #pragma unroll
       for (int u = 0; u < U; ++u) {
@@ -145,6 +156,11 @@ __global__ void __launch_bounds__(kTile, 3) adj_fwd_kernel(const AdjFwdArgs a) {
           w = fmaxf(w_min, fminf(w_max, w));
           a.w_out[base + 32 * (k0 + u)] = w;
         }
+      }
+#pragma unroll
+      for (int u = 0; u < U; ++u) {
+        p[u] = pn[u];
+        wv[u] = wn[u];
       }
     }
   }
@@ -355,6 +371,8 @@ __global__ void __launch_bounds__(kTile, 3) adj_bwd_kernel(const AdjBwdArgs a) {
     const long long s = nd.slice_base + (slice_row0 >> 5);
     const int len = a.sl_len[s];
     const long long base = a.sl_off[s] + lane;
+    // all U entries' stream loads, then all gathers, before the dependent
+    // math (measured faster here than a software pipeline of the groups)
     constexpr int U = 8;
     for (int k0 = 0; k0 < len; k0 += U) {
       uint32_t p[U];
