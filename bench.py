@@ -261,6 +261,39 @@ def fp64_error_small():
 
 
 # ---------------------------------------------------------------------------
+# plain engine, small (N=1000, k=20): latency-bound, reported in us/step
+# ---------------------------------------------------------------------------
+def run_small(args):
+    import torch
+
+    from leviathan_v1_b200 import LeviathanEngine
+    from leviathan_v1_b200.graphs import config_small
+
+    net = config_small(0)
+    e = LeviathanEngine(*net.engine_args())
+    e.autotune(DT, trial_steps=10)  # chooses the cluster path or graph replay
+    info = e.cluster_info()
+    stream = torch.cuda.ExternalStream(e.stream_ptr)
+    steps = 500
+    e.step_n_async(DT, steps)
+    e.synchronize()
+    ev0 = torch.cuda.Event(enable_timing=True)
+    ev1 = torch.cuda.Event(enable_timing=True)
+    ev0.record(stream)
+    e.step_n_async(DT, steps)
+    ev1.record(stream)
+    ev1.synchronize()
+    ms = ev0.elapsed_time(ev1)
+    e.close()
+    return {"workload": "Watts-Strogatz N=1000, k=20, p=0.1, delays U[1,50], 500 steps, "
+                        "controller on",
+            "N": net.N, "E": net.E, "steps": steps, "us_per_step": ms * 1e3 / steps,
+            "edge_updates_per_s": net.E * steps / (ms / 1e3),
+            "path": ("cluster-resident kernel, %d CTAs" % info["ctas"]) if info["enabled"]
+                    else "step kernel graph replay"}
+
+
+# ---------------------------------------------------------------------------
 # batched sweep (512 networks, one launch per step, sharded over ranks)
 # ---------------------------------------------------------------------------
 def run_batched(args, rank, world, plain_value):
@@ -562,6 +595,8 @@ def run_ours(args, rank, world, local):
     }
     if not args.no_batched:
         line["batched"] = run_batched(args, rank, world, value)
+    if rank == 0:
+        line["small"] = run_small(args)
     if rank == 0 and not args.no_adjoint:
         line["adjoint"] = run_adjoint(args)
         line["reservoir"] = run_reservoir(args)
