@@ -172,6 +172,11 @@ struct LevEngine {
   float2 *d_pend = nullptr;  // [total_nodes] parked (coupling sum, eps)
   int *d_class_nets = nullptr;  // networks of each class, class by class
   LevHubs *hubs = nullptr;      // attached hub monitor (lev_attach_hubs)
+  // step blocks of engines with several degree classes: one chain of
+  // launches per class, forked from and joined back to `stream` in the graph
+  cudaStream_t class_stream[kNumClasses] = {nullptr, nullptr, nullptr};
+  cudaEvent_t ev_fork = nullptr;
+  cudaEvent_t ev_join[kNumClasses] = {nullptr, nullptr, nullptr};
 
   // r of the last single step, written by the kernel into mapped host memory
   float *h_rmap = nullptr;
@@ -253,6 +258,11 @@ void free_engine(LevEngine *h) {
   cudaFree(h->d_rhist);
   if (h->h_rmap) cudaFreeHost(h->h_rmap);
   if (h->h_rstage) cudaFreeHost(h->h_rstage);
+  for (int c = 0; c < kNumClasses; ++c) {
+    if (h->class_stream[c]) cudaStreamDestroy(h->class_stream[c]);
+    if (h->ev_join[c]) cudaEventDestroy(h->ev_join[c]);
+  }
+  if (h->ev_fork) cudaEventDestroy(h->ev_fork);
   if (h->stream) cudaStreamDestroy(h->stream);
   delete h;
 }
@@ -360,15 +370,16 @@ int prepare_step_kernels() {
   return LEV_OK;
 }
 
-int launch_class(LevEngine *h, int c, StepArgs a) {
+int launch_class(LevEngine *h, int c, StepArgs a, cudaStream_t s = nullptr) {
   const TileClass &tc = h->classes[c];
   if (tc.ntiles == 0) return LEV_OK;
+  if (!s) s = h->stream;
   a.tiles = h->d_tiles + tc.tile_off;
   const int mode = (h->math_mode == LEV_MATH_ACCURATE) ? 1 : 0;
   void *args[] = {&a};
   LEV_TRY_CUDA(cudaLaunchKernel(
       reinterpret_cast<const void *>(kVariants[tc.variant].fn[mode]),
-      dim3(tc.ntiles), dim3(kTile), args, 0, h->stream));
+      dim3(tc.ntiles), dim3(kTile), args, 0, s));
   return LEV_OK;
 }
 
@@ -400,9 +411,10 @@ bool pairs_active(const LevEngine *h) {
 
 // phase 0: pair_kernel (or a first step_kernel for a class without a pair
 // variant); phase 1: finish_kernel (or a second step_kernel).
-int launch_pair_class(LevEngine *h, int c, StepArgs a, int phase) {
+int launch_pair_class(LevEngine *h, int c, StepArgs a, int phase, cudaStream_t s = nullptr) {
   const TileClass &tc = h->classes[c];
   if (tc.ntiles == 0) return LEV_OK;
+  if (!s) s = h->stream;
   a.tiles = h->d_tiles + tc.tile_off;
   const int mode = (h->math_mode == LEV_MATH_ACCURATE) ? 1 : 0;
   if (tc.pair_variant < 0 || phase == 0) {
@@ -411,17 +423,17 @@ int launch_pair_class(LevEngine *h, int c, StepArgs a, int phase) {
             ? reinterpret_cast<const void *>(kVariants[tc.variant].fn[mode])
             : reinterpret_cast<const void *>(kPairVariants[tc.pair_variant].fn[mode]);
     void *args[] = {&a};
-    LEV_TRY_CUDA(cudaLaunchKernel(fn, dim3(tc.ntiles), dim3(kTile), args, 0, h->stream));
+    LEV_TRY_CUDA(cudaLaunchKernel(fn, dim3(tc.ntiles), dim3(kTile), args, 0, s));
   } else {
     const int blocks = (tc.ntiles + kFinishTiles - 1) / kFinishTiles;
     if (mode)
-      finish_kernel<1><<<blocks, kTile, 0, h->stream>>>(a, tc.ntiles);
+      finish_kernel<1><<<blocks, kTile, 0, s>>>(a, tc.ntiles);
     else
-      finish_kernel<0><<<blocks, kTile, 0, h->stream>>>(a, tc.ntiles);
+      finish_kernel<0><<<blocks, kTile, 0, s>>>(a, tc.ntiles);
     LEV_TRY_CUDA(cudaGetLastError());
   }
   if (tc.pair_variant >= 0) {  // r and g of the class's networks
-    reduce_kernel<<<tc.nnets, kReduceThreads, 0, h->stream>>>(a, h->d_class_nets + tc.net_off);
+    reduce_kernel<<<tc.nnets, kReduceThreads, 0, s>>>(a, h->d_class_nets + tc.net_off);
     LEV_TRY_CUDA(cudaGetLastError());
   }
   return LEV_OK;
@@ -466,13 +478,44 @@ int get_graph(LevEngine *h, int len, float dt, cudaGraphExec_t *out) {
   StepArgs a = make_args(h, dt, h->d_rhist, h->block_len, nullptr);
   int rc = LEV_OK;
   const bool pairs = pairs_active(h);
-  for (int i = 0; i < len && rc == LEV_OK;) {
-    if (pairs && i + 1 < len) {
-      rc = launch_two_steps(h, a);
-      i += 2;
-    } else {
-      rc = launch_step(h, a);
-      i += 1;
+  int busy[kNumClasses], nbusy = 0;
+  for (int c = 0; c < kNumClasses; ++c)
+    if (h->classes[c].ntiles > 0) busy[nbusy++] = c;
+  if (nbusy > 1 && h->ev_fork) {
+    // the classes' networks are independent: one chain per class, so the
+    // classes' launches overlap instead of queueing behind each other
+    LEV_TRY_CUDA(cudaEventRecord(h->ev_fork, h->stream));
+    const int sweep0 = h->sweep;
+    for (int q = 0; q < nbusy; ++q) {
+      const int c = busy[q];
+      cudaStream_t cs = h->class_stream[c];
+      if (rc == LEV_OK && cudaStreamWaitEvent(cs, h->ev_fork, 0) != cudaSuccess)
+        rc = fail(LEV_ERR_CUDA, "graph fork failed");
+      int sweep = sweep0;
+      const bool two = pairs && h->classes[c].pair_variant >= 0;
+      for (int i = 0; i < len && rc == LEV_OK;) {
+        const int n = (two && i + 1 < len) ? 2 : 1;
+        for (int phase = 0; phase < n && rc == LEV_OK; ++phase) {
+          a.reverse = sweep;
+          sweep ^= 1;
+          rc = (n == 2) ? launch_pair_class(h, c, a, phase, cs) : launch_class(h, c, a, cs);
+        }
+        i += n;
+      }
+      // join every chain that was forked, even after a failure
+      cudaEventRecord(h->ev_join[c], cs);
+      cudaStreamWaitEvent(h->stream, h->ev_join[c], 0);
+      h->sweep = sweep;
+    }
+  } else {
+    for (int i = 0; i < len && rc == LEV_OK;) {
+      if (pairs && i + 1 < len) {
+        rc = launch_two_steps(h, a);
+        i += 2;
+      } else {
+        rc = launch_step(h, a);
+        i += 1;
+      }
     }
   }
   cudaError_t ce = cudaStreamEndCapture(h->stream, &ge.graph);
@@ -816,6 +859,18 @@ int create_impl(LevEngine **out, int num_nets, const int32_t *Ns,
   }
   int rc = prepare_step_kernels();
   setup_cluster(h, h_sl_off, h_sl_len);
+  {
+    int nbusy = 0;
+    for (int c = 0; c < kNumClasses; ++c) nbusy += h->classes[c].ntiles > 0;
+    if (nbusy > 1) {
+      bool ok = cudaEventCreateWithFlags(&h->ev_fork, cudaEventDisableTiming) == cudaSuccess;
+      for (int c = 0; c < kNumClasses && ok; ++c)
+        ok = cudaStreamCreateWithFlags(&h->class_stream[c], cudaStreamNonBlocking) ==
+                 cudaSuccess &&
+             cudaEventCreateWithFlags(&h->ev_join[c], cudaEventDisableTiming) == cudaSuccess;
+      if (!ok) rc = fail(LEV_ERR_CUDA, "class streams: creation failed");
+    }
+  }
 #define LEV_ALLOC(ptr, count)                      \
   if (rc == LEV_OK) rc = dev_alloc(h, &(ptr), (count));
   LEV_ALLOC(h->d_nets, (size_t)num_nets);
