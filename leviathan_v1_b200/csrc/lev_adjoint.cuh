@@ -296,8 +296,10 @@ __device__ __forceinline__ int pos_mod(long long x, int m) {
   return r < 0 ? r + m : r;
 }
 
-template <int MATH>
-__global__ void __launch_bounds__(kTile, 3) adj_bwd_kernel(const AdjBwdArgs a) {
+// U: edges per lane whose loads are in flight together; MINB: resident CTAs
+// per SM the register budget is sized for.
+template <int MATH, int U, int MINB>
+__global__ void __launch_bounds__(kTile, MINB) adj_bwd_kernel(const AdjBwdArgs a) {
   __shared__ float s_red[32];
   __shared__ int s_last;
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
@@ -373,7 +375,6 @@ __global__ void __launch_bounds__(kTile, 3) adj_bwd_kernel(const AdjBwdArgs a) {
     const long long base = a.sl_off[s] + lane;
     // all U entries' stream loads, then all gathers, before the dependent
     // math (measured faster here than a software pipeline of the groups)
-    constexpr int U = 8;
     for (int k0 = 0; k0 < len; k0 += U) {
       uint32_t p[U];
       float wv[U], lw[U], dj[U];

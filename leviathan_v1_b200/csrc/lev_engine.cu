@@ -2660,10 +2660,16 @@ int lev_adj_backward(LevAdjoint *a, const float *dLdr, const float *dLdtheta,
         b.grad_ra = a->res_gra;
         b.grad_rb = a->res_grb;
       }
-      if (mode)
-        adj_bwd_kernel<1><<<e->total_tiles, kTile, 0, s>>>(b);
-      else
-        adj_bwd_kernel<0><<<e->total_tiles, kTile, 0, s>>>(b);
+      // measured on B200: grids of many waves (batch-64 reservoir) run best
+      // at 4 CTAs/SM with 4 edges in flight per lane, a grid of one partial
+      // wave (N = 10^4) at 3 CTAs/SM with 8
+      if (e->total_tiles > 3 * 148 * 2) {
+        if (mode) adj_bwd_kernel<1, 4, 4><<<e->total_tiles, kTile, 0, s>>>(b);
+        else adj_bwd_kernel<0, 4, 4><<<e->total_tiles, kTile, 0, s>>>(b);
+      } else {
+        if (mode) adj_bwd_kernel<1, 8, 3><<<e->total_tiles, kTile, 0, s>>>(b);
+        else adj_bwd_kernel<0, 8, 3><<<e->total_tiles, kTile, 0, s>>>(b);
+      }
       LEV_TRY_CUDA(cudaGetLastError());
     }
     if (overlap) {
