@@ -178,14 +178,21 @@ def _ref_engine(net, flavor="sm100a"):
     return RefEngine(*net.engine_args(), flavor=flavor)
 
 
+@pytest.mark.parametrize("blocks", [False, True], ids=["step", "step_n"])
 @pytest.mark.parametrize("N,k,md,steps", [(20_000, 16, 30, 60), (100_000, 32, 64, 20),
-                                          (1_000_000, 32, 64, 5)])
-def test_engine_matches_live_reference(N, k, md, steps):
+                                          (1_000_000, 32, 64, 6)])
+def test_engine_matches_live_reference(N, k, md, steps, blocks):
+    """Against the reference engine itself on the same GPU; ``step_n``
+    takes two steps per launch (pair and finish kernels)."""
     net = make_network(N, k, 0.1, md, seed=N)
     ref = _ref_engine(net)
     eng = LeviathanEngine(*net.engine_args())
     r_ref = ref.run(DT, steps)
-    r_eng = np.array([eng.step(DT) for _ in range(steps)], np.float32)
+    if blocks:
+        assert eng.pair_info()[0]["eligible"]
+        r_eng = eng.step_n(DT, steps)
+    else:
+        r_eng = np.array([eng.step(DT) for _ in range(steps)], np.float32)
     s = ref.state()
     _cmp("r", r_eng, r_ref, REF_TOL["r"])
     _cmp("theta@", eng.get_theta(), s["theta"], REF_TOL["theta"])
