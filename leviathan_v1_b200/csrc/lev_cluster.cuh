@@ -4,7 +4,7 @@
 // A network of up to 16 x 1024 nodes whose edges, node state and delay ring
 // fit in the shared memory of one thread-block cluster (up to 16 CTAs, one per
 // SM, 227 KB each) is stepped n times in ONE launch:
-//   * CTA r of the cluster owns rows [r*R, r*R + R), R a multiple of 256, one
+//   * CTA r of the cluster owns rows [r*R, r*R + R), R a multiple of 32, one
 //     thread per row; its SELL-32 slices (col|delay, weights), its node state
 //     and its rows of every ring slot live in its shared memory;
 //   * a delayed phase of a node owned by another CTA is read from that CTA's
@@ -12,10 +12,13 @@
 //   * one cluster barrier per step orders every ring write before the next
 //     step's reads (with max_delay+2 ring slots, reads and the write of one
 //     step never touch the same slot);
-//   * each 256-node block's (sum cos, sum sin) goes to a double-buffered
-//     array in CTA 0; after the barrier every CTA reduces them in the
-//     reference's order (leviathan_kernel.cu:242-263), so all CTAs compute
-//     the same r and gain without a second barrier.
+//   * each warp's shuffle-tree (sum cos, sum sin) of its 32 rows goes to a
+//     double-buffered array in CTA 0; after the barrier every CTA forms the
+//     256-node block sums from eight warp sums with the arithmetic of the
+//     reference's block tree (leviathan_kernel.cu:198-233) and reduces the
+//     blocks in the order of :242-263, so all CTAs compute the same r and
+//     gain without a second barrier.  A 256-node block may thus span CTAs,
+//     and a small network spreads over up to 16 SMs.
 // Arithmetic and summation order are those of step_kernel: results are
 // bitwise the same as stepping with step_kernel.
 
@@ -25,7 +28,46 @@ namespace lev {
 
 constexpr int kClusterMax = 16;     // CTAs per cluster (non-portable size)
 constexpr int kClusterRowsMax = 1024;
-constexpr int kClusterBlocksMax = kClusterMax * kClusterRowsMax / kTile;  // 64
+constexpr int kClusterWarpsMax = kClusterMax * kClusterRowsMax / 32;  // 512
+
+// Sum of one 256-node block from its eight warp sums v[0..7], with the
+// arithmetic of the reference's second-level tree (leviathan_kernel.cu:
+// 216-233: warp 0 takes the eight warp sums in lanes 0-7, zeros elsewhere,
+// then shuffle-down adds at offsets 16, 8, 4, 2, 1): the first two levels add
+// zeros (which turns -0 into +0), then (v0+v4, ...), then pairs, then one.
+__device__ __forceinline__ float block_tree8(const float *v) {
+  float z[8];
+#pragma unroll
+  for (int i = 0; i < 8; ++i) z[i] = __fadd_rn(__fadd_rn(v[i], 0.0f), 0.0f);
+  const float a0 = __fadd_rn(z[0], z[4]), a1 = __fadd_rn(z[1], z[5]);
+  const float a2 = __fadd_rn(z[2], z[6]), a3 = __fadd_rn(z[3], z[7]);
+  return __fadd_rn(__fadd_rn(a0, a2), __fadd_rn(a1, a3));
+}
+
+// r of one step from the warp sums wsum[nwarps_blocks * 8] (one warp: lane l
+// adds blocks l, l+32, ..., then the shuffle tree), as final_reduce_r_kernel
+// (leviathan_kernel.cu:242-263) over the reference's block partials.
+__device__ __forceinline__ float2 cluster_sums(const float2 *wsum, int nblocks, int lane) {
+  float sum_cos = 0.0f, sum_sin = 0.0f;
+  for (int b = lane; b < nblocks; b += 32) {
+    float vc[8], vs[8];
+#pragma unroll
+    for (int i = 0; i < 8; ++i) {
+      const float2 v = wsum[b * 8 + i];
+      vc[i] = v.x;
+      vs[i] = v.y;
+    }
+    sum_cos += block_tree8(vc);
+    sum_sin += block_tree8(vs);
+  }
+  const unsigned mask = 0xffffffffu;
+#pragma unroll
+  for (int off = 16; off > 0; off /= 2) {
+    sum_cos += __shfl_down_sync(mask, sum_cos, off);
+    sum_sin += __shfl_down_sync(mask, sum_sin, off);
+  }
+  return make_float2(sum_cos, sum_sin);
+}
 
 struct ClusterArgs {
   const NetDesc *net;
@@ -49,7 +91,7 @@ struct ClusterArgs {
 };
 
 // shared memory layout (bytes, from the dynamic base):
-//   part   float2 [2][kClusterBlocksMax]       block partials (used in CTA 0)
+//   wsum   float2 [2][kClusterWarpsMax]        warp sums (used in CTA 0)
 //   sloff  int    [R/32]   slice start (relative to the CTA's first entry)
 //   sllen  int    [R/32]
 //   th, thh, om, omh  float [R]
@@ -61,8 +103,6 @@ __global__ void __launch_bounds__(kClusterRowsMax, 1) cluster_kernel(const Clust
   namespace cg = cooperative_groups;
   cg::cluster_group cluster = cg::this_cluster();
   extern __shared__ __align__(16) unsigned char smem[];
-  __shared__ float s_rc[32];
-  __shared__ float s_rs[32];
 
   const NetDesc nd = *a.net;
   const int rank = (int)cluster.block_rank();
@@ -74,8 +114,8 @@ __global__ void __launch_bounds__(kClusterRowsMax, 1) cluster_kernel(const Clust
   const bool live = (tid < R) && (row < N);
   const int nslices = R / 32;
 
-  float2 *part = reinterpret_cast<float2 *>(smem);
-  int *sloff = reinterpret_cast<int *>(part + 2 * kClusterBlocksMax);
+  float2 *wsum = reinterpret_cast<float2 *>(smem);
+  int *sloff = reinterpret_cast<int *>(wsum + 2 * kClusterWarpsMax);
   int *sllen = sloff + nslices;
   float *s_th = reinterpret_cast<float *>(sllen + nslices);
   float *s_thh = s_th + R;
@@ -121,31 +161,25 @@ __global__ void __launch_bounds__(kClusterRowsMax, 1) cluster_kernel(const Clust
   int cur = ns.cur, rbuf = ns.rbuf;
   float g = ns.g, r = ns.r;
   const int nblocks = (N + kTile - 1) / kTile;
+  // warps past the network's last row contribute zero sums to their block
+  if (rank == 0)
+    for (int k = tid; k < 2 * kClusterWarpsMax; k += blockDim.x) wsum[k] = make_float2(0.0f, 0.0f);
   const float dt = a.dt;
   const float eta = nd.eta, gamma = nd.gamma, lam = nd.lam;
   const float w_min = nd.w_min, w_max = nd.w_max;
   const unsigned mask = 0xffffffffu;
   cluster.sync();
 
-  float2 *part0 = cluster.map_shared_rank(part, 0);
+  float2 *wsum0 = cluster.map_shared_rank(wsum, 0);
   __shared__ float s_g;
   for (int step = 0; step < a.n_steps; ++step) {
     // ---- r and gain of the previous step: warp 0 of every CTA reduces the
     // block partials (same order everywhere) and shares g with its CTA ----
     if (step > 0) {
       if (warp == 0) {
-        const float2 *pb = part0 + ((step - 1) & 1) * kClusterBlocksMax;
-        float sum_cos = 0.0f, sum_sin = 0.0f;
-        for (int k = lane; k < nblocks; k += 32) {
-          const float2 v = pb[k];
-          sum_cos += v.x;
-          sum_sin += v.y;
-        }
-#pragma unroll
-        for (int off = 16; off > 0; off /= 2) {
-          sum_cos += __shfl_down_sync(mask, sum_cos, off);
-          sum_sin += __shfl_down_sync(mask, sum_sin, off);
-        }
+        const float2 sums =
+            cluster_sums(wsum0 + ((step - 1) & 1) * kClusterWarpsMax, nblocks, lane);
+        const float sum_cos = sums.x, sum_sin = sums.y;
         if (lane == 0) {
           float inv_N = 1.0f / (float)N;
           r = sqrtf(sum_cos * sum_cos + sum_sin * sum_sin) * inv_N;
@@ -230,50 +264,25 @@ __global__ void __launch_bounds__(kClusterRowsMax, 1) cluster_kernel(const Clust
       s_ring[(size_t)nxt * R + tid] = x;
       lev_sincos<MATH>(x, &my_sin, &my_cos);
     }
-    // ---- 256-node block partials (leviathan_kernel.cu:198-233) --------------
+    // ---- warp sums of (cos, sin), first level of the block tree
+    // (leviathan_kernel.cu:198-214), to CTA 0 ------------------------------
 #pragma unroll
     for (int off = 16; off > 0; off /= 2) {
       my_cos += __shfl_down_sync(mask, my_cos, off);
       my_sin += __shfl_down_sync(mask, my_sin, off);
     }
-    if (lane == 0) {
-      s_rc[warp] = my_cos;
-      s_rs[warp] = my_sin;
-    }
-    __syncthreads();
-    if ((warp & 7) == 0 && warp * 32 < R) {  // first warp of each 256-row block
-      const int b = warp >> 3;                // block within this CTA
-      float c = (lane < 8) ? s_rc[warp + lane] : 0.0f;
-      float s = (lane < 8) ? s_rs[warp + lane] : 0.0f;
-#pragma unroll
-      for (int off = 16; off > 0; off /= 2) {
-        c += __shfl_down_sync(mask, c, off);
-        s += __shfl_down_sync(mask, s, off);
-      }
-      const int gb = row0 / kTile + b;
-      if (lane == 0 && gb < nblocks)
-        part0[(step & 1) * kClusterBlocksMax + gb] = make_float2(c, s);
-    }
+    if (lane == 0)
+      wsum0[(step & 1) * kClusterWarpsMax + row0 / 32 + warp] = make_float2(my_cos, my_sin);
     cur = nxt;
     rbuf = (rbuf + 1 == nd.max_delay + 1) ? 0 : rbuf + 1;
     cluster.sync();
   }
   // ---- r of the last step, then write the state back ------------------------
   if (a.n_steps > 0) {
-    const float2 *pb = part0 + ((a.n_steps - 1) & 1) * kClusterBlocksMax;
-    float sum_cos = 0.0f, sum_sin = 0.0f;
-    for (int k = lane; k < nblocks; k += 32) {
-      const float2 v = pb[k];
-      sum_cos += v.x;
-      sum_sin += v.y;
-    }
-#pragma unroll
-    for (int off = 16; off > 0; off /= 2) {
-      sum_cos += __shfl_down_sync(mask, sum_cos, off);
-      sum_sin += __shfl_down_sync(mask, sum_sin, off);
-    }
-    sum_cos = __shfl_sync(mask, sum_cos, 0);
-    sum_sin = __shfl_sync(mask, sum_sin, 0);
+    const float2 sums =
+        cluster_sums(wsum0 + ((a.n_steps - 1) & 1) * kClusterWarpsMax, nblocks, lane);
+    const float sum_cos = __shfl_sync(mask, sums.x, 0);
+    const float sum_sin = __shfl_sync(mask, sums.y, 0);
     float inv_N = 1.0f / (float)N;
     r = sqrtf(sum_cos * sum_cos + sum_sin * sum_sin) * inv_N;
     if (nd.ctrl) g = gain_controller(g, r, dt, nd);

@@ -591,7 +591,8 @@ void setup_cluster(LevEngine *h, const std::vector<long long> &sl_off,
   if (cudaDeviceGetAttribute(&max_smem, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev) !=
       cudaSuccess)
     return;
-  for (int R = kTile; R <= kClusterRowsMax; R += kTile) {
+  // the smallest rows-per-CTA that fits (up to 16 CTAs): the most SMs
+  for (int R = 32; R <= kClusterRowsMax; R += 32) {
     const int C = (d.N + R - 1) / R;
     if (C > kClusterMax) continue;
     long long cap = 0;
@@ -601,7 +602,7 @@ void setup_cluster(LevEngine *h, const std::vector<long long> &sl_off,
         e += 32LL * sl_len[d.slice_base + s];
       cap = std::max(cap, e);
     }
-    const size_t smem = sizeof(float2) * 2 * kClusterBlocksMax + sizeof(int) * 2 * (R / 32) +
+    const size_t smem = sizeof(float2) * 2 * kClusterWarpsMax + sizeof(int) * 2 * (R / 32) +
                         sizeof(float) * 4 * R + sizeof(float) * (size_t)d.bsi * R +
                         8 * (size_t)cap;
     if (smem + 1024 > (size_t)max_smem) continue;
@@ -636,9 +637,10 @@ void setup_cluster(LevEngine *h, const std::vector<long long> &sl_off,
     h->cluster_C = C;
     h->cluster_edge_cap = (int)cap;
     h->cluster_smem = smem;
-    // measured on B200: faster than per-step graph replay up to ~8 CTAs of
-    // distributed gathers; lev_autotune times both and decides per engine
-    h->use_cluster = C <= 8;
+    // measured on B200: faster than per-step graph replay up to 256 rows per
+    // CTA (N = 4096 on 16 CTAs), slower at 1024; lev_autotune times both
+    // and decides per engine
+    h->use_cluster = R <= 256;
     return;
   }
 }

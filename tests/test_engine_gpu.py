@@ -277,6 +277,7 @@ def test_cluster_path_bit_identical(N, k, md, ctrl):
     b = LeviathanEngine(*net.engine_args(), params=dict(gain_controller=ctrl))
     info = a.cluster_info()
     assert info["eligible"], info
+    a.set_cluster_mode(True)
     b.set_cluster_mode(False)
     ra = np.concatenate([a.step_n(DT, 5), a.step_n(DT, 300)])
     rb = np.concatenate([b.step_n(DT, 5), b.step_n(DT, 300)])
