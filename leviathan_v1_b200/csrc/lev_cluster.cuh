@@ -85,7 +85,8 @@ struct ClusterArgs {
   float *r_hist;  // [n] (row rpos + k), or null
   int r_cap;
   int n_steps;
-  int R;          // rows per CTA (multiple of 256)
+  int R;          // rows per CTA (a power of two, 32 .. 1024)
+  int lgR;        // log2(R)
   int edge_cap;   // SELL entries per CTA the shared memory was sized for
   float dt;
 };
@@ -98,8 +99,10 @@ struct ClusterArgs {
 //   ring   float  [bsi][R]
 //   cd     uint32 [edge_cap]
 //   w      float  [edge_cap]
-template <int MATH>
-__global__ void __launch_bounds__(kClusterRowsMax, 1) cluster_kernel(const ClusterArgs a) {
+// MAXR: largest rows per CTA of the instantiation (the register budget);
+// U: edges per lane whose gathers are in flight together.
+template <int MATH, int MAXR, int U>
+__global__ void __launch_bounds__(MAXR, 1) cluster_kernel(const ClusterArgs a) {
   namespace cg = cooperative_groups;
   cg::cluster_group cluster = cg::this_cluster();
   extern __shared__ __align__(16) unsigned char smem[];
@@ -212,7 +215,6 @@ __global__ void __launch_bounds__(kClusterRowsMax, 1) cluster_kernel(const Clust
     if (warp < my_slices) {
       const int len = sllen[warp];
       const int base = sloff[warp] + lane;
-      constexpr int U = 8;
       for (int k0 = 0; k0 < len; k0 += U) {
         uint32_t p[U];
         float wv[U], dj[U];
@@ -227,8 +229,8 @@ __global__ void __launch_bounds__(kClusterRowsMax, 1) cluster_kernel(const Clust
           int slot = cur - (int)(p[u] & 255u);
           slot += (slot < 0) ? bsi : 0;
           const int j = (int)(p[u] >> 8);
-          const int owner = j / R;
-          const int loc = j - owner * R;
+          const int owner = j >> a.lgR;
+          const int loc = j & (R - 1);
           const float *src = (owner == rank) ? s_ring : cluster.map_shared_rank(s_ring, owner);
           dj[u] = src[(size_t)slot * R + loc];
         }

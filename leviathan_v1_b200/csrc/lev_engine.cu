@@ -537,6 +537,15 @@ int get_graph(LevEngine *h, int len, float dt, cudaGraphExec_t *out) {
   return LEV_OK;
 }
 
+// Cluster kernel instantiation for R rows per CTA: up to 256 rows the
+// register budget allows 24 edges in flight per lane, above it 8.
+using ClusterFn = void (*)(ClusterArgs);
+ClusterFn cluster_fn(int R, int math_mode) {
+  const bool acc = math_mode == LEV_MATH_ACCURATE;
+  if (R <= 256) return acc ? cluster_kernel<1, 256, 24> : cluster_kernel<0, 256, 24>;
+  return acc ? cluster_kernel<1, kClusterRowsMax, 8> : cluster_kernel<0, kClusterRowsMax, 8>;
+}
+
 // One launch of the cluster-resident kernel: `len` steps, r history rows
 // 0..len-1 in d_rhist.
 int launch_cluster(LevEngine *h, float dt, int len) {
@@ -558,6 +567,8 @@ int launch_cluster(LevEngine *h, float dt, int len) {
   ca.r_cap = h->block_len;
   ca.n_steps = len;
   ca.R = h->cluster_R;
+  ca.lgR = 0;
+  while ((1 << ca.lgR) < h->cluster_R) ++ca.lgR;
   ca.edge_cap = h->cluster_edge_cap;
   ca.dt = dt;
   cudaLaunchConfig_t cfg = {};
@@ -572,10 +583,7 @@ int launch_cluster(LevEngine *h, float dt, int len) {
   attr[0].val.clusterDim.z = 1;
   cfg.attrs = attr;
   cfg.numAttrs = 1;
-  if (h->math_mode == LEV_MATH_ACCURATE)
-    LEV_TRY_CUDA(cudaLaunchKernelEx(&cfg, cluster_kernel<1>, ca));
-  else
-    LEV_TRY_CUDA(cudaLaunchKernelEx(&cfg, cluster_kernel<0>, ca));
+  LEV_TRY_CUDA(cudaLaunchKernelEx(&cfg, cluster_fn(h->cluster_R, h->math_mode), ca));
   return LEV_OK;
 }
 
@@ -592,7 +600,7 @@ void setup_cluster(LevEngine *h, const std::vector<long long> &sl_off,
       cudaSuccess)
     return;
   // the smallest rows-per-CTA that fits (up to 16 CTAs): the most SMs
-  for (int R = 32; R <= kClusterRowsMax; R += 32) {
+  for (int R = 32; R <= kClusterRowsMax; R *= 2) {
     const int C = (d.N + R - 1) / R;
     if (C > kClusterMax) continue;
     long long cap = 0;
@@ -608,8 +616,8 @@ void setup_cluster(LevEngine *h, const std::vector<long long> &sl_off,
     if (smem + 1024 > (size_t)max_smem) continue;
     bool ok = true;
     for (int m = 0; m < 2 && ok; ++m) {
-      const void *fn = m ? reinterpret_cast<const void *>(cluster_kernel<1>)
-                         : reinterpret_cast<const void *>(cluster_kernel<0>);
+      const void *fn = reinterpret_cast<const void *>(
+          cluster_fn(R, m ? LEV_MATH_ACCURATE : LEV_MATH_REFERENCE));
       ok = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) ==
                cudaSuccess &&
            cudaFuncSetAttribute(fn, cudaFuncAttributeNonPortableClusterSizeAllowed, 1) ==
