@@ -459,6 +459,186 @@ __global__ void __launch_bounds__(kTile, MINB) adj_bwd_kernel(const AdjBwdArgs a
   }
 }
 
+// The reverse step with LPR lanes per row, for grids that leave most SMs idle
+// with one lane per row (N ~ 10^4: 40 CTAs on 148 SMs).  Each 256-row tile is
+// taken by LPR CTAs of 256/LPR rows; lane q of a row walks the row's SELL
+// entries q, q + LPR, ...; the row's sums (coupling sum S_i, the lam_D sum, the
+// |eps| term) are combined by shuffles and the node-level work is done by the
+// row's first lane.  The per-edge arithmetic is that of adj_bwd_kernel; only
+// the order of the sums over a row's edges differs (the gradients agree to
+// rounding).  Partials: LPR per tile.
+template <int MATH, int LPR, int U>
+__global__ void __launch_bounds__(kTile, 4) adj_bwd_split_kernel(const AdjBwdArgs a) {
+  constexpr int RPC = kTile / LPR;  // rows per CTA
+  __shared__ float s_red[32];
+  __shared__ int s_last;
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const int sub = blockIdx.x % LPR;
+  const int2 tile = a.tiles[blockIdx.x / LPR];
+  const NetDesc nd = a.nets[tile.x];
+  const int q = tid % LPR;
+  const int N = nd.N, row0 = tile.y, row = row0 + sub * RPC + tid / LPR;
+  const bool live = row < N;
+  const long long gi = nd.node_off + row;
+  const float dt = a.dt;
+  const int Np = nd.Np;
+  const int bsa = nd.max_delay + 2;
+  const int hs = (int)(a.s - a.seg_start) + nd.max_delay;  // history slot of theta(s)
+  const float *H = a.H + nd.ring_off;
+  float *AR = a.adj_ring + nd.aux_off;
+  const int as_next = pos_mod(a.s + 1, bsa);
+  const int as_s = pos_mod(a.s, bsa);
+  const unsigned mask = 0xffffffffu;
+
+  const float4 tr = a.trace[tile.x];
+  const float g_s = tr.x, r1 = tr.y;
+  float dgdr = 0.0f, dgdg = 1.0f;
+  if (nd.ctrl) {
+    const float pre = g_s + dt * (nd.beta * (nd.r0 - r1) - nd.mu * (g_s - nd.g_rest));
+    const bool free = pre >= nd.g_min && pre <= nd.g_max;
+    dgdr = free ? -dt * nd.beta : 0.0f;
+    dgdg = free ? 1.0f - dt * nd.mu : 0.0f;
+  }
+  const float lam_g1 = a.lam_g[tile.x];
+  const float lam_r = (a.dLdr ? a.dLdr[tile.x] : 0.0f) + lam_g1 * dgdr;
+  const float invN = 1.0f / (float)N;
+  const float Cm = tr.z * invN, Sm = tr.w * invN;
+
+  float lg_part = 0.0f;
+  float lt1 = 0.0f, th = 0.0f, eps = 0.0f, diff = 0.0f;
+  int deg = 0;
+  if (live) {
+    th = H[(long long)hs * Np + row];
+    diff = wrap_pm_pi(th - a.thh_s[gi]);
+    eps = sinf(diff);
+    const int *rp = a.row_ptr + nd.rp_off + row;
+    deg = rp[1] - rp[0];
+    if (q == 0) {
+      // (A) adjoint of theta(s+1), complete; (B) integrate
+      const float th1 = H[(long long)(hs + 1) * Np + row];
+      float *slot_next = AR + (long long)as_next * Np + row;
+      lt1 = a.lam_th[gi] + *slot_next;
+      *slot_next = 0.0f;
+      float sn, cs;
+      sincosf(th1, &sn, &cs);
+      if (r1 > 0.0f) lt1 += lam_r * (Sm * cs - Cm * sn) * invN / r1;
+      if (a.dLdth) lt1 += a.dLdth[gi];
+      if (a.dLdy) {
+        const float gy = a.dLdy[tile.x];
+        lt1 += gy * (a.rb[gi] * cs - a.ra[gi] * sn);
+        a.grad_ra[gi] += gy * cs;
+        a.grad_rb[gi] += gy * sn;
+      }
+      a.grad_omega[gi] += lt1 * dt;
+      if (a.grad_drive) a.grad_drive[gi] = lt1 * dt;
+      if (a.grad_win) a.grad_win[gi] += lt1 * dt * a.xin[tile.x];
+    }
+  }
+  lt1 = __shfl_sync(mask, lt1, lane & ~(LPR - 1));  // from the row's first lane
+  const float lam_S = lt1 * dt * g_s;
+  const float ae = fabsf(eps);
+  const float eta = nd.eta, gamma = nd.gamma, lam = nd.lam;
+  const float w_min = nd.w_min, w_max = nd.w_max;
+  const float decay = 1.0f - dt * lam;
+  float S_i = 0.0f, lsum = 0.0f, labs = 0.0f;
+  // the warp's rows lie in one 32-row SELL slice (32 / LPR consecutive rows)
+  const int wrow0 = row0 + sub * RPC + warp * (32 / LPR);
+  if (wrow0 < N) {
+    const long long s = nd.slice_base + (wrow0 >> 5);
+    const int len = a.sl_len[s];
+    const long long base = a.sl_off[s] + (row & 31);
+    for (int kb = 0; kb < len; kb += LPR * U) {
+      uint32_t p[U];
+      float wv[U], lw[U], dj[U];
+#pragma unroll
+      for (int u = 0; u < U; ++u) {
+        const int k = kb + LPR * u + q;
+        const bool in = k < deg;
+        p[u] = in ? __ldg(a.sl_cd + base + 32 * k) : 0u;
+        wv[u] = in ? a.w_s[base + 32 * k] : 0.0f;
+        lw[u] = in ? a.lam_w[base + 32 * k] : 0.0f;
+      }
+#pragma unroll
+      for (int u = 0; u < U; ++u) {
+        const int d = (int)(p[u] & 255u);
+        dj[u] = H[(long long)(hs - d) * Np + (p[u] >> 8)];
+      }
+#pragma unroll
+      for (int u = 0; u < U; ++u) {
+        const int k = kb + LPR * u + q;
+        if (k < deg) {
+          const int j = (int)(p[u] >> 8), d = (int)(p[u] & 255u);
+          const float delayed_j = dj[u];
+          float dlt = delayed_j - th;
+          dlt = wrap_pm_pi(dlt);
+          const float w = wv[u];
+          float sn, cs;
+          lev_sincos<MATH>(dlt, &sn, &cs);
+          S_i += w * sn;
+          const float w_pre = w + dt * (eta * cs * (1.0f - gamma * ae) - lam * w);
+          const float c = (w_pre >= w_min && w_pre <= w_max) ? 1.0f : 0.0f;
+          const float lwn = lw[u];
+          a.lam_w[base + 32 * k] = lwn * c * decay + lam_S * sn;
+          const float lD = lam_S * w * cs - lwn * c * dt * eta * sn * (1.0f - gamma * ae);
+          labs -= lwn * c * dt * eta * gamma * cs;
+          const int slot = (as_s - d < 0) ? as_s - d + bsa : as_s - d;
+          atomicAdd(AR + (long long)slot * Np + j, lD);
+          lsum -= lD;
+        }
+      }
+    }
+  }
+#pragma unroll
+  for (int off = 1; off < LPR; off *= 2) {
+    S_i += __shfl_xor_sync(mask, S_i, off);
+    lsum += __shfl_xor_sync(mask, lsum, off);
+    labs += __shfl_xor_sync(mask, labs, off);
+  }
+  if (live && q == 0) {
+    // (D) predictor
+    const float sgn = (eps > 0.0f) ? 1.0f : ((eps < 0.0f) ? -1.0f : 0.0f);
+    const float lthh1 = a.lam_thh[gi], lomh1 = a.lam_omh[gi];
+    const float leps = -lt1 * dt * nd.alpha + labs * sgn + lomh1 * nd.kappa_w * dt;
+    const float ldiff = leps * cosf(diff);
+    a.lam_th[gi] = lt1 + lsum + ldiff;
+    a.lam_thh[gi] = lthh1 - ldiff;
+    a.lam_omh[gi] = lomh1 + lthh1 * dt;
+    lg_part = lt1 * dt * S_i;
+  }
+  // (E) lam_g(s) = lam_g(s+1) dg/dg + sum_i lam_th'_i dt S_i
+#pragma unroll
+  for (int off = 16; off > 0; off /= 2) lg_part += __shfl_down_sync(mask, lg_part, off);
+  if (lane == 0) s_red[warp] = lg_part;
+  __syncthreads();
+  const int nparts = nd.ntiles * LPR;
+  if (warp == 0) {
+    lg_part = (lane < kTile / 32) ? s_red[lane] : 0.0f;
+#pragma unroll
+    for (int off = 16; off > 0; off /= 2) lg_part += __shfl_down_sync(mask, lg_part, off);
+    if (lane == 0) {
+      a.partials[(long long)nd.part_off * LPR + (row0 / kTile) * LPR + sub] =
+          make_float2(lg_part, 0.0f);
+      __threadfence();
+      const unsigned prev = atomicAdd(a.tickets + tile.x, 1u);
+      s_last = (prev == (unsigned)(nparts - 1));
+    }
+  }
+  __syncthreads();
+  if (!s_last) return;
+  __threadfence();
+  if (warp == 0) {
+    float sum = 0.0f;
+    const float2 *part = a.partials + (long long)nd.part_off * LPR;
+    for (int k = lane; k < nparts; k += 32) sum += __ldcg(part + k).x;
+#pragma unroll
+    for (int off = 16; off > 0; off /= 2) sum += __shfl_down_sync(mask, sum, off);
+    if (lane == 0) {
+      a.lam_g[tile.x] = lam_g1 * dgdg + sum;
+      a.tickets[tile.x] = 0u;
+    }
+  }
+}
+
 // Checkpoint of the ring window of every network: mode 0 saves theta(t-m),
 // m = 0..max_delay, from the ring (slot (cur - m) mod bsi) into
 // ck[m][N] (per network at ck_off); mode 1 writes it back as

@@ -2413,7 +2413,7 @@ int lev_adj_create(LevAdjoint **out, LevEngine *e, int32_t segment,
   A(a->w, SL);
   A(a->ring, a->ring_floats);
   A(a->partials, e->total_tiles);
-  A(a->bpart, e->total_tiles);
+  A(a->bpart, 4LL * e->total_tiles);  // up to four partials per tile
   A(a->ro_partials, e->total_tiles);
   A(a->tickets, NN);
   A(a->ck_theta, S * TN); A(a->ck_thh, S * TN); A(a->ck_omh, S * TN);
@@ -2671,9 +2671,13 @@ int lev_adj_backward(LevAdjoint *a, const float *dLdr, const float *dLdtheta,
         b.grad_rb = a->res_grb;
       }
       // measured on B200: grids of many waves (batch-64 reservoir) run best
-      // at 4 CTAs/SM with 4 edges in flight per lane, a grid of one partial
-      // wave (N = 10^4) at 3 CTAs/SM with 8
-      if (e->total_tiles > 3 * 148 * 2) {
+      // at 4 CTAs/SM with 4 edges in flight per lane; a grid of one partial
+      // wave (N = 10^4) with four lanes per row
+      if (e->total_tiles <= 148) {
+        const int g4 = e->total_tiles * 4;
+        if (mode) adj_bwd_split_kernel<1, 4, 2><<<g4, kTile, 0, s>>>(b);
+        else adj_bwd_split_kernel<0, 4, 2><<<g4, kTile, 0, s>>>(b);
+      } else if (e->total_tiles > 3 * 148 * 2) {
         if (mode) adj_bwd_kernel<1, 4, 4><<<e->total_tiles, kTile, 0, s>>>(b);
         else adj_bwd_kernel<0, 4, 4><<<e->total_tiles, kTile, 0, s>>>(b);
       } else {
