@@ -254,6 +254,213 @@ __global__ void __launch_bounds__(kTile, 3) adj_fwd_kernel(const AdjFwdArgs a) {
   }
 }
 
+// The forward step with four lanes per row, for grids under one wave
+// (N ~ 10^4: 40 tiles on 148 SMs).  CTA = one 256-row tile, 1024 threads,
+// lanes 4r .. 4r+3 of the CTA on row r.  The row's first lane runs the node
+// work and forms the coupling sum in CSR order from the per-edge terms its
+// three partner lanes and it computed (shuffled), with the same expression;
+// the block trees read the rows' values from shared memory in row order.  So
+// the results are bitwise those of adj_fwd_kernel (and of step_kernel).
+template <int MATH, int U>
+__global__ void __launch_bounds__(4 * kTile, 1) adj_fwd_split_kernel(const AdjFwdArgs a) {
+  constexpr int LPR = 4;
+  __shared__ float s_rc[32];
+  __shared__ float s_rs[32];
+  __shared__ float s_ry[32];
+  __shared__ float s_val[3][kTile];
+  __shared__ int s_last;
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const int q = tid & (LPR - 1);
+  const int rloc = tid / LPR;  // row within the tile
+  const int lead = lane & ~(LPR - 1);
+  const unsigned mask = 0xffffffffu;
+  const int2 tile = a.tiles[blockIdx.x];
+  const NetDesc nd = a.nets[tile.x];
+  NetState *ns = a.st + tile.x;
+  const int N = nd.N, row0 = tile.y, row = row0 + rloc;
+  const bool live = row < N;
+  const long long gi = nd.node_off + row;
+  const float dt = a.dt;
+  const int bsi = nd.bsi, Np = nd.Np, cur = ns->cur;
+  const float g = ns->g;
+  const float *ring = a.ring + nd.ring_off;
+
+  // ---- predictor (row's first lane) ----------------------------------------
+  float th = 0.0f, eps = 0.0f;
+  int deg = 0;
+  if (live) {
+    if (q == 0) {
+      th = a.theta[gi];
+      const float thh = a.theta_hat[gi];
+      const float wh = a.omega_hat[gi];
+      if (a.thh_rec) a.thh_rec[gi] = thh;
+      float diff = th - thh;
+      diff = wrap_pm_pi(diff);
+      eps = sinf(diff);
+      a.theta_hat[gi] = thh + dt * wh;
+      a.omega_hat[gi] = wh + nd.kappa_w * dt * eps;
+    }
+    const int *rp = a.row_ptr + nd.rp_off + row;
+    deg = rp[1] - rp[0];
+  }
+  th = __shfl_sync(mask, th, lead);
+  eps = __shfl_sync(mask, eps, lead);
+  const float my_eps = fabsf(eps);
+  const float eta = nd.eta, gamma = nd.gamma, lam = nd.lam;
+  const float w_min = nd.w_min, w_max = nd.w_max;
+
+  // ---- edges: lane q takes entries q, q+4, ...; the sum in CSR order -------
+  float local_sum = 0.0f;
+  const int wrow0 = row0 + warp * (32 / LPR);  // the warp's 8 rows share a slice
+  if (wrow0 < N) {
+    const long long s = nd.slice_base + (wrow0 >> 5);
+    const int len = a.sl_len[s];
+    const long long base = a.sl_off[s] + (row & 31);
+    for (int kb = 0; kb < len; kb += LPR * U) {
+      uint32_t p[U];
+      float wv[U], dj[U], sn[U];
+#pragma unroll
+      for (int u = 0; u < U; ++u) {
+        const int k = kb + LPR * u + q;
+        const bool in = k < len;
+        p[u] = in ? __ldg(a.sl_cd + base + 32 * k) : 0u;
+        wv[u] = in ? a.w_in[base + 32 * k] : 0.0f;
+      }
+#pragma unroll
+      for (int u = 0; u < U; ++u) {
+        int slot = cur - (int)(p[u] & 255u);
+        slot += (slot < 0) ? bsi : 0;
+        dj[u] = ld_ring(ring + ((unsigned)slot * (unsigned)Np + (p[u] >> 8)));
+      }
+#pragma unroll
+      for (int u = 0; u < U; ++u) {
+        const int k = kb + LPR * u + q;
+        sn[u] = 0.0f;
+        if (k < deg) {
+          const float delayed_j = dj[u];
+          float diff = delayed_j - th;
+          diff = wrap_pm_pi(diff);
+          float w = wv[u];
+          float sin_diff, cos_diff;
+          lev_sincos<MATH>(diff, &sin_diff, &cos_diff);
+          sn[u] = sin_diff;
+          float dw = dt * (eta * cos_diff * (1.0f - gamma * my_eps) - lam * w);
+          w += dw;
+          if (!isfinite(w)) w = w_min;
+          w = fmaxf(w_min, fminf(w_max, w));
+          a.w_out[base + 32 * k] = w;
+        }
+      }
+#pragma unroll
+      for (int e = 0; e < LPR * U; ++e) {
+        const int src = lead + (e % LPR);
+        const float w = __shfl_sync(mask, wv[e / LPR], src);
+        const float sin_diff = __shfl_sync(mask, sn[e / LPR], src);
+        if (kb + e < deg) local_sum += w * sin_diff;  // the expression of adj_fwd_kernel
+      }
+    }
+  }
+
+  // ---- integrate (row's first lane) ----------------------------------------
+  int nxt = cur + 1;
+  if (nxt == bsi) nxt = 0;
+  if (q == 0) {
+    float my_cos = 0.0f, my_sin = 0.0f, my_y = 0.0f;
+    if (live) {
+      float inc;
+      if (a.drive || a.win) {
+        float u = 0.0f;
+        if (a.drive) u += a.drive[gi];
+        if (a.win) u += a.win[gi] * a.xin[tile.x];
+        inc = dt * (a.omega[gi] + g * local_sum - nd.alpha * eps + u);
+      } else {
+        inc = dt * (a.omega[gi] + g * local_sum - nd.alpha * eps);
+      }
+      float x = th + inc;
+      x = wrap_0_2pi(x);
+      if (!isfinite(x)) x = 0.0f;
+      a.theta[gi] = x;
+      if (a.theta_out) a.theta_out[gi] = x;
+      a.ring[nd.ring_off + (long long)nxt * Np + row] = x;
+      lev_sincos<MATH>(x, &my_sin, &my_cos);
+      if (a.ra) my_y = a.ra[gi] * my_cos + a.rb[gi] * my_sin;
+    }
+    s_val[0][rloc] = my_cos;
+    s_val[1][rloc] = my_sin;
+    s_val[2][rloc] = my_y;
+  }
+  __syncthreads();
+
+  // ---- block partials in row order (leviathan_kernel.cu:198-233) -----------
+  if (tid < kTile) {
+    float my_cos = s_val[0][tid], my_sin = s_val[1][tid], my_y = s_val[2][tid];
+#pragma unroll
+    for (int off = 16; off > 0; off /= 2) {
+      my_cos += __shfl_down_sync(mask, my_cos, off);
+      my_sin += __shfl_down_sync(mask, my_sin, off);
+      my_y += __shfl_down_sync(mask, my_y, off);
+    }
+    if (lane == 0) {
+      s_rc[warp] = my_cos;
+      s_rs[warp] = my_sin;
+      s_ry[warp] = my_y;
+    }
+  }
+  __syncthreads();
+  if (warp == 0) {
+    float my_cos = (lane < (kTile / 32)) ? s_rc[lane] : 0.0f;
+    float my_sin = (lane < (kTile / 32)) ? s_rs[lane] : 0.0f;
+    float my_y = (lane < (kTile / 32)) ? s_ry[lane] : 0.0f;
+#pragma unroll
+    for (int off = 16; off > 0; off /= 2) {
+      my_cos += __shfl_down_sync(mask, my_cos, off);
+      my_sin += __shfl_down_sync(mask, my_sin, off);
+      my_y += __shfl_down_sync(mask, my_y, off);
+    }
+    if (lane == 0) {
+      a.partials[nd.part_off + row0 / kTile] = make_float2(my_cos, my_sin);
+      if (a.ra) a.ro_partials[nd.part_off + row0 / kTile] = my_y;
+      __threadfence();
+      const unsigned prev = atomicAdd(&ns->ticket, 1u);
+      s_last = (prev == (unsigned)(nd.ntiles - 1));
+    }
+  }
+  __syncthreads();
+  if (!s_last) return;
+  __threadfence();
+  if (warp == 0) {
+    float sum_cos = 0.0f, sum_sin = 0.0f;
+    const float2 *part = a.partials + nd.part_off;
+    for (int k = lane; k < nd.ntiles; k += 32) {
+      const float2 v = __ldcg(part + k);
+      sum_cos += v.x;
+      sum_sin += v.y;
+    }
+#pragma unroll
+    for (int off = 16; off > 0; off /= 2) {
+      sum_cos += __shfl_down_sync(mask, sum_cos, off);
+      sum_sin += __shfl_down_sync(mask, sum_sin, off);
+    }
+    if (lane == 0) {
+      float inv_N = 1.0f / (float)N;
+      float r = sqrtf(sum_cos * sum_cos + sum_sin * sum_sin) * inv_N;
+      const float gn = nd.ctrl ? gain_controller(g, r, dt, nd) : g;
+      if (a.trace) a.trace[tile.x] = make_float4(g, r, sum_cos, sum_sin);
+      if (a.r_out) a.r_out[tile.x] = r;
+      if (a.ra && a.y_out) {
+        float y = 0.0f;
+        for (int k = 0; k < nd.ntiles; ++k) y += __ldcg(a.ro_partials + nd.part_off + k);
+        a.y_out[tile.x] = y;
+      }
+      ns->g = gn;
+      ns->r = r;
+      ns->cur = nxt;
+      ns->t = ns->t + 1;
+      ns->ticket = 0u;
+    }
+  }
+}
+
 struct AdjBwdArgs {
   const NetDesc *nets;  // adjoint copies (ring_off: history ring, aux_off: adjoint ring)
   const int2 *tiles;

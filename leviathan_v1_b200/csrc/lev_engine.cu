@@ -2322,10 +2322,17 @@ AdjFwdArgs adj_fwd_args(LevAdjoint *a, float dt) {
 int adj_launch_fwd(LevAdjoint *a, const AdjFwdArgs &f, cudaStream_t s = nullptr) {
   LevEngine *e = a->e;
   if (!s) s = e->stream;
-  if (e->math_mode == LEV_MATH_ACCURATE)
+  const bool acc = e->math_mode == LEV_MATH_ACCURATE;
+  if (e->total_tiles <= 148) {  // under one wave: four lanes per row
+    if (acc)
+      adj_fwd_split_kernel<1, 2><<<e->total_tiles, 4 * kTile, 0, s>>>(f);
+    else
+      adj_fwd_split_kernel<0, 2><<<e->total_tiles, 4 * kTile, 0, s>>>(f);
+  } else if (acc) {
     adj_fwd_kernel<1><<<e->total_tiles, kTile, 0, s>>>(f);
-  else
+  } else {
     adj_fwd_kernel<0><<<e->total_tiles, kTile, 0, s>>>(f);
+  }
   LEV_TRY_CUDA(cudaGetLastError());
   return LEV_OK;
 }
