@@ -317,4 +317,254 @@ __global__ void __launch_bounds__(MAXR, 1) cluster_kernel(const ClusterArgs a) {
   cluster.sync();
 }
 
+// The cluster-resident step with four lanes per row (CTA = 4R threads, R up
+// to 128, lanes 4r .. 4r+3 on row r).  The row's first lane runs the node work and forms the
+// coupling sum in CSR order from the per-edge terms the row's lanes computed
+// (shuffled, same expression); the warp-level trees of the block sums read
+// the rows' values from shared memory in row order.  Bitwise the results of
+// cluster_kernel and step_kernel.  Shared memory as cluster_kernel plus
+// ord float [2][R] after omh.
+template <int MATH, int U>
+__global__ void __launch_bounds__(4 * 128, 1) cluster_split_kernel(const ClusterArgs a) {
+  namespace cg = cooperative_groups;
+  constexpr int LPR = 4;
+  cg::cluster_group cluster = cg::this_cluster();
+  extern __shared__ __align__(16) unsigned char smem[];
+
+  const NetDesc nd = *a.net;
+  const int rank = (int)cluster.block_rank();
+  const int R = a.R;
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const int q = tid & (LPR - 1);
+  const int rloc = tid / LPR;
+  const int lead = lane & ~(LPR - 1);
+  const unsigned mask = 0xffffffffu;
+  const int N = nd.N, bsi = nd.bsi, Np = nd.Np;
+  const int row0 = rank * R;
+  const int row = row0 + rloc;
+  const bool live = row < N;
+  const int nslices = R / 32;
+
+  float2 *wsum = reinterpret_cast<float2 *>(smem);
+  int *sloff = reinterpret_cast<int *>(wsum + 2 * kClusterWarpsMax);
+  int *sllen = sloff + nslices;
+  float *s_th = reinterpret_cast<float *>(sllen + nslices);
+  float *s_thh = s_th + R;
+  float *s_om = s_thh + R;
+  float *s_omh = s_om + R;
+  float *s_ord = s_omh + R;
+  float *s_ring = s_ord + 2 * R;
+  uint32_t *s_cd = reinterpret_cast<uint32_t *>(s_ring + (size_t)bsi * R);
+  float *s_w = reinterpret_cast<float *>(s_cd + a.edge_cap);
+
+  // ---- load this CTA's part of the network --------------------------------
+  const long long sl0 = nd.slice_base + row0 / 32;
+  const int my_slices = max(0, min(nslices, (N - row0 + 31) / 32));
+  const long long ebase = my_slices ? a.sl_off[sl0] : 0;
+  long long eend = ebase;
+  for (int s = tid; s < nslices; s += blockDim.x) {
+    if (s < my_slices) {
+      sloff[s] = (int)(a.sl_off[sl0 + s] - ebase);
+      sllen[s] = a.sl_len[sl0 + s];
+    } else {
+      sloff[s] = 0;
+      sllen[s] = 0;
+    }
+  }
+  if (my_slices) eend = a.sl_off[sl0 + my_slices - 1] + 32LL * a.sl_len[sl0 + my_slices - 1];
+  const int nent = (int)(eend - ebase);
+  for (int k = tid; k < nent; k += blockDim.x) {
+    s_cd[k] = a.sl_cd[ebase + k];
+    s_w[k] = a.sl_w[ebase + k];
+  }
+  int deg = 0;
+  if (live) {
+    const long long gi = nd.node_off + row;
+    if (q == 0) {
+      s_th[rloc] = a.theta[gi];
+      s_thh[rloc] = a.theta_hat[gi];
+      s_om[rloc] = a.omega[gi];
+      s_omh[rloc] = a.omega_hat[gi];
+    }
+    const int *rp = a.row_ptr + nd.rp_off + row;
+    deg = rp[1] - rp[0];
+  }
+  for (int s = q; s < bsi; s += LPR)
+    if (live) s_ring[(size_t)s * R + rloc] = a.ring[nd.ring_off + (long long)s * Np + row];
+  NetState ns = *a.st;
+  int cur = ns.cur, rbuf = ns.rbuf;
+  float g = ns.g, r = ns.r;
+  const int nblocks = (N + kTile - 1) / kTile;
+  if (rank == 0)
+    for (int k = tid; k < 2 * kClusterWarpsMax; k += blockDim.x) wsum[k] = make_float2(0.0f, 0.0f);
+  const float dt = a.dt;
+  const float eta = nd.eta, gamma = nd.gamma, lam = nd.lam;
+  const float w_min = nd.w_min, w_max = nd.w_max;
+  // the warp's 8 rows share one SELL slice
+  const int wslice = (warp * (32 / LPR)) / 32;
+  const bool slice_live = row0 + wslice * 32 < N;
+  cluster.sync();
+
+  float2 *wsum0 = cluster.map_shared_rank(wsum, 0);
+  __shared__ float s_g;
+  for (int step = 0; step < a.n_steps; ++step) {
+    if (step > 0) {
+      if (warp == 0) {
+        const float2 sums =
+            cluster_sums(wsum0 + ((step - 1) & 1) * kClusterWarpsMax, nblocks, lane);
+        if (lane == 0) {
+          float inv_N = 1.0f / (float)N;
+          r = sqrtf(sums.x * sums.x + sums.y * sums.y) * inv_N;
+          if (nd.ctrl) g = gain_controller(g, r, dt, nd);
+          s_g = g;
+          if (rank == 0 && a.r_hist) {
+            const int k = ns.rpos + step - 1;
+            if (k < a.r_cap) a.r_hist[k] = r;
+          }
+        }
+      }
+      __syncthreads();
+      g = s_g;
+    }
+    // ---- predictor (row's first lane) --------------------------------------
+    float th = 0.0f, eps = 0.0f;
+    if (live && q == 0) {
+      th = s_th[rloc];
+      const float thh = s_thh[rloc];
+      const float wh = s_omh[rloc];
+      float diff = th - thh;
+      diff = wrap_pm_pi(diff);
+      eps = sinf(diff);
+      s_thh[rloc] = thh + dt * wh;
+      s_omh[rloc] = wh + nd.kappa_w * dt * eps;
+    }
+    th = __shfl_sync(mask, th, lead);
+    eps = __shfl_sync(mask, eps, lead);
+    const float my_eps = fabsf(eps);
+    // ---- edges: lane q takes entries q, q+4, ...; the sum in CSR order -----
+    float local_sum = 0.0f;
+    if (slice_live) {
+      const int len = sllen[wslice];
+      const int base = sloff[wslice] + (rloc & 31);
+      for (int kb = 0; kb < len; kb += LPR * U) {
+        uint32_t p[U];
+        float wv[U], dj[U], sn[U];
+#pragma unroll
+        for (int u = 0; u < U; ++u) {
+          const int k = kb + LPR * u + q;
+          const bool in = k < deg;
+          p[u] = in ? s_cd[base + 32 * k] : 0u;
+          wv[u] = in ? s_w[base + 32 * k] : 0.0f;
+        }
+#pragma unroll
+        for (int u = 0; u < U; ++u) {
+          int slot = cur - (int)(p[u] & 255u);
+          slot += (slot < 0) ? bsi : 0;
+          const int j = (int)(p[u] >> 8);
+          const int owner = j >> a.lgR;
+          const int loc = j & (R - 1);
+          const float *src = (owner == rank) ? s_ring : cluster.map_shared_rank(s_ring, owner);
+          dj[u] = src[(size_t)slot * R + loc];
+        }
+#pragma unroll
+        for (int u = 0; u < U; ++u) {
+          const int k = kb + LPR * u + q;
+          sn[u] = 0.0f;
+          if (k < deg) {
+            const float delayed_j = dj[u];
+            float diff = delayed_j - th;
+            diff = wrap_pm_pi(diff);
+            float w = wv[u];
+            float sin_diff, cos_diff;
+            lev_sincos<MATH>(diff, &sin_diff, &cos_diff);
+            sn[u] = sin_diff;
+            float dw = dt * (eta * cos_diff * (1.0f - gamma * my_eps) - lam * w);
+            w += dw;
+            if (!isfinite(w)) w = w_min;
+            w = fmaxf(w_min, fminf(w_max, w));
+            s_w[base + 32 * k] = w;
+          }
+        }
+#pragma unroll
+        for (int e = 0; e < LPR * U; ++e) {
+          const int srcl = lead + (e % LPR);
+          const float w = __shfl_sync(mask, wv[e / LPR], srcl);
+          const float sin_diff = __shfl_sync(mask, sn[e / LPR], srcl);
+          if (kb + e < deg) local_sum += w * sin_diff;  // the expression of cluster_kernel
+        }
+      }
+    }
+    // ---- integrate (row's first lane) --------------------------------------
+    int nxt = cur + 1;
+    if (nxt == bsi) nxt = 0;
+    if (q == 0) {
+      float my_cos = 0.0f, my_sin = 0.0f;
+      if (live) {
+        float inc = dt * (s_om[rloc] + g * local_sum - nd.alpha * eps);
+        float x = th + inc;
+        x = wrap_0_2pi(x);
+        if (!isfinite(x)) x = 0.0f;
+        s_th[rloc] = x;
+        s_ring[(size_t)nxt * R + rloc] = x;
+        lev_sincos<MATH>(x, &my_sin, &my_cos);
+      }
+      s_ord[rloc] = my_cos;
+      s_ord[R + rloc] = my_sin;
+    }
+    __syncthreads();
+    // ---- warp sums in row order to CTA 0 (leviathan_kernel.cu:198-214) ----
+    if (tid < R) {
+      float c = s_ord[tid], sn = s_ord[R + tid];
+#pragma unroll
+      for (int off = 16; off > 0; off /= 2) {
+        c += __shfl_down_sync(mask, c, off);
+        sn += __shfl_down_sync(mask, sn, off);
+      }
+      if (lane == 0)
+        wsum0[(step & 1) * kClusterWarpsMax + row0 / 32 + warp] = make_float2(c, sn);
+    }
+    cur = nxt;
+    rbuf = (rbuf + 1 == nd.max_delay + 1) ? 0 : rbuf + 1;
+    cluster.sync();
+  }
+  // ---- r of the last step, then write the state back ------------------------
+  if (a.n_steps > 0) {
+    const float2 sums =
+        cluster_sums(wsum0 + ((a.n_steps - 1) & 1) * kClusterWarpsMax, nblocks, lane);
+    const float sum_cos = __shfl_sync(mask, sums.x, 0);
+    const float sum_sin = __shfl_sync(mask, sums.y, 0);
+    float inv_N = 1.0f / (float)N;
+    r = sqrtf(sum_cos * sum_cos + sum_sin * sum_sin) * inv_N;
+    if (nd.ctrl) g = gain_controller(g, r, dt, nd);
+    if (rank == 0 && tid == 0) {
+      if (a.r_hist) {
+        const int k = ns.rpos + a.n_steps - 1;
+        if (k < a.r_cap) a.r_hist[k] = r;
+      }
+      NetState o = ns;
+      o.g = g;
+      o.r = r;
+      o.cur = cur;
+      o.rbuf = rbuf;
+      o.t = ns.t + a.n_steps;
+      o.rpos = ns.rpos + a.n_steps;
+      o.ticket = 0u;
+      *a.st = o;
+    }
+  }
+  if (live) {
+    const long long gi = nd.node_off + row;
+    if (q == 0) {
+      a.theta[gi] = s_th[rloc];
+      a.theta_hat[gi] = s_thh[rloc];
+      a.omega_hat[gi] = s_omh[rloc];
+    }
+    for (int s = q; s < bsi; s += LPR)
+      a.ring[nd.ring_off + (long long)s * Np + row] = s_ring[(size_t)s * R + rloc];
+  }
+  for (int k = tid; k < nent; k += blockDim.x) a.sl_w[ebase + k] = s_w[k];
+  // no CTA may leave while a peer can still read its shared memory
+  cluster.sync();
+}
+
 }  // namespace lev

@@ -537,14 +537,17 @@ int get_graph(LevEngine *h, int len, float dt, cudaGraphExec_t *out) {
   return LEV_OK;
 }
 
-// Cluster kernel instantiation for R rows per CTA: up to 256 rows the
-// register budget allows 24 edges in flight per lane, above it 8.
+// Cluster kernel for R rows per CTA (measured on B200): up to 128 rows four
+// lanes per row (4R threads); 256 rows one lane per row with 24 gathers in
+// flight; above, one lane per row with 8.
 using ClusterFn = void (*)(ClusterArgs);
 ClusterFn cluster_fn(int R, int math_mode) {
   const bool acc = math_mode == LEV_MATH_ACCURATE;
+  if (R <= 128) return acc ? cluster_split_kernel<1, 8> : cluster_split_kernel<0, 8>;
   if (R <= 256) return acc ? cluster_kernel<1, 256, 24> : cluster_kernel<0, 256, 24>;
   return acc ? cluster_kernel<1, kClusterRowsMax, 8> : cluster_kernel<0, kClusterRowsMax, 8>;
 }
+inline int cluster_threads(int R) { return R <= 128 ? 4 * R : R; }
 
 // One launch of the cluster-resident kernel: `len` steps, r history rows
 // 0..len-1 in d_rhist.
@@ -573,7 +576,7 @@ int launch_cluster(LevEngine *h, float dt, int len) {
   ca.dt = dt;
   cudaLaunchConfig_t cfg = {};
   cfg.gridDim = dim3(h->cluster_C);
-  cfg.blockDim = dim3(h->cluster_R);
+  cfg.blockDim = dim3(cluster_threads(h->cluster_R));
   cfg.dynamicSmemBytes = h->cluster_smem;
   cfg.stream = h->stream;
   cudaLaunchAttribute attr[1];
@@ -611,8 +614,8 @@ void setup_cluster(LevEngine *h, const std::vector<long long> &sl_off,
       cap = std::max(cap, e);
     }
     const size_t smem = sizeof(float2) * 2 * kClusterWarpsMax + sizeof(int) * 2 * (R / 32) +
-                        sizeof(float) * 4 * R + sizeof(float) * (size_t)d.bsi * R +
-                        8 * (size_t)cap;
+                        sizeof(float) * (R <= 128 ? 6 : 4) * R +
+                        sizeof(float) * (size_t)d.bsi * R + 8 * (size_t)cap;
     if (smem + 1024 > (size_t)max_smem) continue;
     bool ok = true;
     for (int m = 0; m < 2 && ok; ++m) {
@@ -625,7 +628,7 @@ void setup_cluster(LevEngine *h, const std::vector<long long> &sl_off,
       if (ok) {
         cudaLaunchConfig_t cfg = {};
         cfg.gridDim = dim3(C);
-        cfg.blockDim = dim3(R);
+        cfg.blockDim = dim3(cluster_threads(R));
         cfg.dynamicSmemBytes = smem;
         cudaLaunchAttribute attr[1];
         attr[0].id = cudaLaunchAttributeClusterDimension;
