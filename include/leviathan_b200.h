@@ -244,6 +244,21 @@ int lev_cluster_info(const LevEngine *h, int32_t *eligible, int32_t *enabled,
                      int32_t *ctas, int32_t *rows_per_cta, int64_t *smem_bytes);
 int lev_set_cluster_mode(LevEngine *h, int32_t enabled);
 
+/* Grid-resident path (no reference counterpart): a single network whose CTAs
+ * (64, 128 or 256 rows each, four lanes per row, its edges and node state in
+ * shared memory) can all be resident at once is stepped by lev_step_n /
+ * lev_step_n_async with one cooperative launch per block of steps; the delay
+ * ring stays in global memory (L2) and one grid barrier orders each step.
+ * The barrier wait is bounded; a timeout makes lev_step_n / lev_sync return
+ * LEV_ERR_CUDA and disables the path.  Results are bitwise those of the
+ * per-step kernel.  The cluster path takes precedence when both are enabled.
+ * lev_grid_info: rows_per_cta in use; eligible_rows_mask = OR of the
+ * eligible rows-per-CTA values.  lev_set_grid_mode: enabled 0 forces the
+ * per-step kernel; rows_per_cta 0 keeps the current choice. */
+int lev_grid_info(const LevEngine *h, int32_t *eligible, int32_t *enabled, int32_t *ctas,
+                  int32_t *rows_per_cta, int64_t *smem_bytes, int32_t *eligible_rows_mask);
+int lev_set_grid_mode(LevEngine *h, int32_t enabled, int32_t rows_per_cta);
+
 /* Two steps per launch (no reference counterpart).  When no delay of the
  * engine is 0, step t+1's predictor and edge work need only the row's own
  * theta(t+1) and ring slots written before step t, so step blocks

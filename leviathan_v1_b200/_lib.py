@@ -102,6 +102,9 @@ PROTOTYPES = {
     "lev_cluster_info": (C.c_int, [_P, C.POINTER(_i32), C.POINTER(_i32),
                                    C.POINTER(_i32), C.POINTER(_i32), C.POINTER(_i64)]),
     "lev_set_cluster_mode": (C.c_int, [_P, _i32]),
+    "lev_grid_info": (C.c_int, [_P, C.POINTER(_i32), C.POINTER(_i32), C.POINTER(_i32),
+                                C.POINTER(_i32), C.POINTER(_i64), C.POINTER(_i32)]),
+    "lev_set_grid_mode": (C.c_int, [_P, _i32, _i32]),
     "lev_num_pair_variants": (C.c_int, []),
     "lev_pair_variant_info": (C.c_int, [_i32, C.POINTER(_i32), C.POINTER(_i32),
                                         C.POINTER(_i32)]),

@@ -22,6 +22,7 @@
 #include "lev_kernels.cuh"
 #include "lev_pair.cuh"
 #include "lev_cluster.cuh"
+#include "lev_grid.cuh"  // uses cluster_sums from lev_cluster.cuh
 
 namespace lev {
 
@@ -197,6 +198,19 @@ struct LevEngine {
   bool use_cluster = true;   // may step blocks use it
   int cluster_R = 0, cluster_C = 0, cluster_edge_cap = 0;
   size_t cluster_smem = 0;
+
+  // grid-resident path for mid-sized single networks (lev_grid.cuh): one
+  // cooperative launch per step block, rows per CTA 64, 128 or 256
+  bool grid_ok = false;      // some rows-per-CTA choice is eligible
+  bool use_grid = true;      // may step blocks use it
+  int grid_R = 0;            // rows per CTA in use
+  bool grid_R_ok[3] = {false, false, false};  // R = 64, 128, 256
+  int grid_cap[3] = {0, 0, 0};                // SELL entries per CTA
+  size_t grid_smem_R[3] = {0, 0, 0};
+  int grid_nwarps = 0;
+  float2 *d_gwsum = nullptr;  // [2][grid_nwarps]
+  unsigned *d_gbar = nullptr;
+  int *h_gerr = nullptr, *d_gerr = nullptr;  // barrier timeout flag (mapped)
 };
 
 struct LeviathanHandle {
@@ -256,6 +270,9 @@ void free_engine(LevEngine *h) {
   cudaFree(h->d_pend);
   cudaFree(h->d_class_nets);
   cudaFree(h->d_rhist);
+  cudaFree(h->d_gwsum);
+  cudaFree(h->d_gbar);
+  if (h->h_gerr) cudaFreeHost(h->h_gerr);
   if (h->h_rmap) cudaFreeHost(h->h_rmap);
   if (h->h_rstage) cudaFreeHost(h->h_rstage);
   for (int c = 0; c < kNumClasses; ++c) {
@@ -656,6 +673,139 @@ void setup_cluster(LevEngine *h, const std::vector<long long> &sl_off,
   }
 }
 
+// Grid kernel for R rows per CTA (64, 128, 256), four lanes per row.
+using GridFn = void (*)(GridArgs);
+constexpr int kGridRs[3] = {64, 128, 256};
+GridFn grid_fn(int R, int math_mode) {
+  const bool acc = math_mode == LEV_MATH_ACCURATE;
+  if (R == 64) return acc ? grid_kernel<1, 64, 8> : grid_kernel<0, 64, 8>;
+  if (R == 128) return acc ? grid_kernel<1, 128, 8> : grid_kernel<0, 128, 8>;
+  return acc ? grid_kernel<1, 256, 8> : grid_kernel<0, 256, 8>;
+}
+inline int grid_r_index(int R) { return R == 64 ? 0 : (R == 128 ? 1 : 2); }
+
+// One cooperative launch of the grid-resident kernel: `len` steps, r history
+// rows 0..len-1 in d_rhist.
+int launch_grid(LevEngine *h, float dt, int len) {
+  reset_rpos_kernel<<<1, 128, 0, h->stream>>>(h->d_st, h->num_nets);
+  LEV_TRY_CUDA(cudaMemsetAsync(h->d_gbar, 0, sizeof(unsigned), h->stream));
+  const int R = h->grid_R, ri = grid_r_index(R);
+  GridArgs ga;
+  ga.net = h->d_nets;
+  ga.st = h->d_st;
+  ga.row_ptr = h->d_row_ptr;
+  ga.sl_off = h->d_sl_off;
+  ga.sl_len = h->d_sl_len;
+  ga.sl_cd = h->d_sl_cd;
+  ga.sl_w = h->d_sl_w;
+  ga.theta = h->d_theta;
+  ga.theta_hat = h->d_theta_hat;
+  ga.omega = h->d_omega;
+  ga.omega_hat = h->d_omega_hat;
+  ga.ring = h->d_ring;
+  ga.wsum = h->d_gwsum;
+  ga.bar = h->d_gbar;
+  ga.early = h->pair_ok ? 1 : 0;  // no delay is 0
+  ga.err = h->d_gerr;
+  ga.r_hist = h->d_rhist;
+  ga.r_cap = h->block_len;
+  ga.n_steps = len;
+  ga.nwarps = h->grid_nwarps;
+  ga.edge_cap = h->grid_cap[ri];
+  ga.dt = dt;
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3((h->h_nets[0].N + R - 1) / R);
+  cfg.blockDim = dim3(kGridLPR * R);
+  cfg.dynamicSmemBytes = h->grid_smem_R[ri];
+  cfg.stream = h->stream;
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeCooperative;
+  attr[0].val.cooperative = 1;
+  cfg.attrs = attr;
+  cfg.numAttrs = 1;
+  LEV_TRY_CUDA(cudaLaunchKernelEx(&cfg, grid_fn(R, h->math_mode), ga));
+  return LEV_OK;
+}
+
+// Mid-sized single networks: for each rows-per-CTA choice, check that every
+// CTA of the grid kernel can be resident at once (shared memory, occupancy,
+// cooperative launch).  Allocates the warp sums, barrier and error flag.
+int setup_grid(LevEngine *h, const std::vector<long long> &sl_off,
+               const std::vector<int> &sl_len) {
+  h->grid_ok = false;
+  if (h->num_nets != 1) return LEV_OK;
+  const NetDesc &d = h->h_nets[0];
+  int dev = 0, max_smem = 0, coop = 0, sms = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess ||
+      cudaDeviceGetAttribute(&max_smem, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev) !=
+          cudaSuccess ||
+      cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, dev) != cudaSuccess ||
+      cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess) {
+    cudaGetLastError();
+    return LEV_OK;
+  }
+  if (!coop) return LEV_OK;
+  const int nblocks = (d.N + kTile - 1) / kTile;
+  const int nwarps = 8 * nblocks;
+  for (int ri = 0; ri < 3; ++ri) {
+    const int R = kGridRs[ri];
+    const int C = (d.N + R - 1) / R;
+    if (C < 2) continue;  // one CTA: the cluster path or graph replay
+    long long cap = 0;
+    for (int c = 0; c < C; ++c) {
+      long long e = 0;
+      for (int s = c * R / 32; s < std::min<long long>((c + 1) * R / 32, (d.N + 31) / 32); ++s)
+        e += 32LL * sl_len[d.slice_base + s];
+      cap = std::max(cap, e);
+    }
+    const size_t smem = sizeof(float2) * nwarps + sizeof(float) * 6 * R +
+                        sizeof(int) * 2 * (R / 32) + 8 * (size_t)cap;
+    if (smem + 1024 > (size_t)max_smem) continue;
+    bool ok = true;
+    for (int m = 0; m < 2 && ok; ++m) {
+      const void *fn = reinterpret_cast<const void *>(
+          grid_fn(R, m ? LEV_MATH_ACCURATE : LEV_MATH_REFERENCE));
+      int per_sm = 0;
+      ok = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) ==
+               cudaSuccess &&
+           cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, kGridLPR * R, smem) ==
+               cudaSuccess &&
+           (long long)per_sm * sms >= C;
+    }
+    cudaGetLastError();  // clear a refused attribute, if any
+    if (!ok) continue;
+    h->grid_R_ok[ri] = true;
+    h->grid_cap[ri] = (int)cap;
+    h->grid_smem_R[ri] = smem;
+    if (!h->grid_ok) h->grid_R = R;  // the smallest: the most SMs
+    h->grid_ok = true;
+  }
+  if (!h->grid_ok) return LEV_OK;
+  h->grid_nwarps = nwarps;
+  int rc = dev_alloc(h, &h->d_gwsum, 2 * (size_t)nwarps);
+  if (rc == LEV_OK) rc = dev_alloc(h, &h->d_gbar, 1);
+  if (rc != LEV_OK) return rc;
+  LEV_TRY_CUDA(cudaMemset(h->d_gwsum, 0, sizeof(float2) * 2 * (size_t)nwarps));
+  LEV_TRY_CUDA(cudaHostAlloc(reinterpret_cast<void **>(&h->h_gerr), sizeof(int),
+                             cudaHostAllocMapped));
+  *h->h_gerr = 0;
+  LEV_TRY_CUDA(cudaHostGetDevicePointer(reinterpret_cast<void **>(&h->d_gerr), h->h_gerr, 0));
+  return LEV_OK;
+}
+
+// After the stream has drained: a grid barrier that timed out leaves the
+// engine state undefined; report it once and stop using the grid path.
+int check_grid_error(LevEngine *h) {
+  if (h->h_gerr && *reinterpret_cast<volatile int *>(h->h_gerr)) {
+    *h->h_gerr = 0;
+    h->grid_ok = false;
+    return fail(LEV_ERR_CUDA,
+                "grid-resident step block: a grid barrier wait timed out; the engine state "
+                "is undefined");
+  }
+  return LEV_OK;
+}
+
 // Enqueue n steps as graph replays (or cluster-kernel launches for small
 // networks); if stage != null, the r history of every block is copied into
 // stage[n][num_nets] (pinned host memory).
@@ -665,6 +815,9 @@ int enqueue_steps(LevEngine *h, float dt, int n, float *stage) {
     const int len = std::min(h->block_len, n - done);
     if (h->cluster_ok && h->use_cluster && !h->hubs) {
       int rc = launch_cluster(h, dt, len);
+      if (rc != LEV_OK) return rc;
+    } else if (h->grid_ok && h->use_grid && !h->hubs) {
+      int rc = launch_grid(h, dt, len);
       if (rc != LEV_OK) return rc;
     } else {
       cudaGraphExec_t ex;
@@ -872,6 +1025,7 @@ int create_impl(LevEngine **out, int num_nets, const int32_t *Ns,
   }
   int rc = prepare_step_kernels();
   setup_cluster(h, h_sl_off, h_sl_len);
+  if (rc == LEV_OK) rc = setup_grid(h, h_sl_off, h_sl_len);
   {
     int nbusy = 0;
     for (int c = 0; c < kNumClasses; ++c) nbusy += h->classes[c].ntiles > 0;
@@ -1168,6 +1322,8 @@ int lev_step_n(LevEngine *h, float dt, int32_t n, float *r_out) {
   int rc = enqueue_steps(h, dt, n, stage);
   if (rc != LEV_OK) return rc;
   LEV_TRY_CUDA(cudaStreamSynchronize(h->stream));
+  rc = check_grid_error(h);
+  if (rc != LEV_OK) return rc;
   if (r_out)
     std::memcpy(r_out, stage, sizeof(float) * (size_t)n * h->num_nets);
   return LEV_OK;
@@ -1185,7 +1341,7 @@ int lev_sync(LevEngine *h) {
   if (!h) return fail(LEV_ERR_ARG, "null handle");
   DeviceScope ds(h->device);
   LEV_TRY_CUDA(cudaStreamSynchronize(h->stream));
-  return LEV_OK;
+  return check_grid_error(h);
 }
 
 int lev_get_stream(LevEngine *h, void **stream) {
@@ -1541,6 +1697,38 @@ int lev_set_cluster_mode(LevEngine *h, int32_t enabled) {
   return LEV_OK;
 }
 
+int lev_grid_info(const LevEngine *h, int32_t *eligible, int32_t *enabled, int32_t *ctas,
+                  int32_t *rows_per_cta, int64_t *smem_bytes, int32_t *eligible_rows_mask) {
+  if (!h) return fail(LEV_ERR_ARG, "null handle");
+  const int R = h->grid_R;
+  const int ri = grid_r_index(R);
+  if (eligible) *eligible = h->grid_ok ? 1 : 0;
+  if (enabled) *enabled = h->use_grid ? 1 : 0;
+  if (ctas) *ctas = (h->grid_ok && R > 0) ? (h->h_nets[0].N + R - 1) / R : 0;
+  if (rows_per_cta) *rows_per_cta = h->grid_ok ? R : 0;
+  if (smem_bytes) *smem_bytes = h->grid_ok ? (int64_t)h->grid_smem_R[ri] : 0;
+  if (eligible_rows_mask) {
+    int m = 0;
+    for (int i = 0; i < 3; ++i)
+      if (h->grid_R_ok[i]) m |= kGridRs[i];
+    *eligible_rows_mask = m;
+  }
+  return LEV_OK;
+}
+
+int lev_set_grid_mode(LevEngine *h, int32_t enabled, int32_t rows_per_cta) {
+  if (!h) return fail(LEV_ERR_ARG, "null handle");
+  if (rows_per_cta != 0) {
+    if (rows_per_cta != 64 && rows_per_cta != 128 && rows_per_cta != 256)
+      return fail(LEV_ERR_ARG, "rows_per_cta must be 0, 64, 128 or 256");
+    if (!h->grid_R_ok[grid_r_index(rows_per_cta)])
+      return fail(LEV_ERR_ARG, "rows_per_cta not eligible for this engine");
+    h->grid_R = rows_per_cta;
+  }
+  h->use_grid = enabled != 0;
+  return LEV_OK;
+}
+
 int lev_num_variants(void) { return kNumVariants; }
 
 int lev_num_pair_variants(void) { return kNumPairVariants; }
@@ -1802,21 +1990,38 @@ int lev_autotune(LevEngine *h, float dt, int32_t trial_steps,
     g_tune_cache[tune_key(tc, c)] = best_v;
     if (h->pair_ok) g_pair_cache[tune_key(tc, c)] = tc.pair_variant;
   }
-  // small single networks: cluster-resident kernel or per-step graph replay
-  if (rc == LEV_OK && h->cluster_ok) {
+  // small and mid-sized single networks: per-step graph replay, the
+  // cluster-resident kernel or the grid-resident kernel (each rows-per-CTA
+  // choice), whichever is fastest
+  if (rc == LEV_OK && (h->cluster_ok || h->grid_ok)) {
     const int n = std::max(trial_steps, 32);
-    float t_mode[2] = {0.0f, 0.0f};
-    for (int m = 1; m >= 0 && rc == LEV_OK; --m) {
+    // mode 0: graph replay, 1: cluster, 2 + ri: grid with kGridRs[ri]
+    float best_t = -1.0f;
+    int best_m = 0;
+    for (int m = 0; m < 5 && rc == LEV_OK; ++m) {
+      if (m == 1 && !h->cluster_ok) continue;
+      if (m >= 2 && !h->grid_R_ok[m - 2]) continue;
       h->use_cluster = (m == 1);
+      h->use_grid = (m >= 2);
+      if (m >= 2) h->grid_R = kGridRs[m - 2];
       rc = enqueue_steps(h, dt, n, nullptr);  // warm-up (graph instantiation)
       if (rc != LEV_OK) break;
       cudaEventRecord(e0, h->stream);
       rc = enqueue_steps(h, dt, n, nullptr);
       cudaEventRecord(e1, h->stream);
-      if (rc == LEV_OK && cudaEventSynchronize(e1) == cudaSuccess)
-        cudaEventElapsedTime(&t_mode[m], e0, e1);
+      float t = 0.0f;
+      if (rc == LEV_OK && cudaEventSynchronize(e1) == cudaSuccess &&
+          cudaEventElapsedTime(&t, e0, e1) == cudaSuccess) {
+        if (best_t < 0.0f || t < best_t) {
+          best_t = t;
+          best_m = m;
+        }
+      }
+      if (rc == LEV_OK) rc = check_grid_error(h);
     }
-    h->use_cluster = rc == LEV_OK && t_mode[1] <= t_mode[0];
+    h->use_cluster = rc == LEV_OK && best_m == 1;
+    h->use_grid = rc == LEV_OK && best_m >= 2;
+    if (best_m >= 2) h->grid_R = kGridRs[best_m - 2];
   }
   if (e0) cudaEventDestroy(e0);
   if (e1) cudaEventDestroy(e1);

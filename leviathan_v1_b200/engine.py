@@ -291,6 +291,21 @@ class _EngineBase:
     def set_cluster_mode(self, enabled: bool) -> None:
         check(self._lib.lev_set_cluster_mode(self.handle, 1 if enabled else 0))
 
+    # -- grid-resident path (mid-sized single networks) --------------------
+    def grid_info(self) -> dict:
+        el, en, c, r, m = (C.c_int32() for _ in range(5))
+        sm = C.c_int64()
+        check(self._lib.lev_grid_info(self.handle, C.byref(el), C.byref(en), C.byref(c),
+                                      C.byref(r), C.byref(sm), C.byref(m)))
+        rows = [R for R in (64, 128, 256) if m.value & R]
+        return dict(eligible=bool(el.value), enabled=bool(en.value), ctas=c.value,
+                    rows_per_cta=r.value, smem_bytes=sm.value, eligible_rows=rows)
+
+    def set_grid_mode(self, enabled: bool, rows_per_cta: int = 0) -> None:
+        """Allow (or forbid) the grid-resident path for step blocks;
+        rows_per_cta 64, 128 or 256 picks the CTA size (0 keeps it)."""
+        check(self._lib.lev_set_grid_mode(self.handle, 1 if enabled else 0, int(rows_per_cta)))
+
     # -- two steps per launch (step blocks; no zero delays) -----------------
     def pair_info(self) -> list:
         """Per degree class: whether two steps per launch are possible

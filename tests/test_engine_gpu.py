@@ -137,14 +137,23 @@ def _replay_blocks(e, actions, record, dt):
 
 @pytest.mark.skipif(not golden_cases(), reason="golden vectors not generated")
 @pytest.mark.parametrize("case", golden_cases() or ["none"])
-def test_step_blocks_bit_identical_to_reference_golden(case):
-    """Step blocks (graph replay; two steps per launch where no delay is 0)
-    reproduce the reference engine bit for bit, including blocks of odd
-    length and blocks interrupted by set_theta / gain / controller calls."""
+@pytest.mark.parametrize("path", ["graph", "cluster", "grid"])
+def test_step_blocks_bit_identical_to_reference_golden(case, path):
+    """Step blocks (graph replay with two steps per launch where no delay is
+    0, the cluster-resident kernel, the grid-resident kernel) reproduce the
+    reference engine bit for bit, including blocks of odd length and blocks
+    interrupted by set_theta / gain / controller calls."""
     z = load_golden(case)
     net = network_from_golden(z)
     e = LeviathanEngine(*net.engine_args())
-    e.set_cluster_mode(False)
+    e.set_cluster_mode(path == "cluster")
+    e.set_grid_mode(path == "grid")
+    if path == "cluster" and not e.cluster_info()["eligible"]:
+        e.close()
+        pytest.skip("cluster path not eligible")
+    if path == "grid" and not e.grid_info()["eligible"]:
+        e.close()
+        pytest.skip("grid path not eligible")
     assert e.pair_info()[0]["eligible"] == bool(np.all(net.delays > 0))
     rs, snaps = _replay_blocks(e, decode_actions(z), record_from_golden(z), float(z["dt"]))
     e.close()
@@ -279,6 +288,7 @@ def test_cluster_path_bit_identical(N, k, md, ctrl):
     assert info["eligible"], info
     a.set_cluster_mode(True)
     b.set_cluster_mode(False)
+    b.set_grid_mode(False)
     ra = np.concatenate([a.step_n(DT, 5), a.step_n(DT, 300)])
     rb = np.concatenate([b.step_n(DT, 5), b.step_n(DT, 300)])
     np.testing.assert_array_equal(ra, rb)
@@ -296,6 +306,50 @@ def test_cluster_path_bit_identical(N, k, md, ctrl):
     assert a.step(DT) == b.step(DT)
     a.close()
     b.close()
+
+
+@pytest.mark.parametrize("N,k,md,ctrl,mode", [(10_000, 20, 50, 1, "reference"),
+                                              (10_000, 20, 50, 1, "accurate"),
+                                              (3000, 12, 0, 1, "reference"),
+                                              (20_000, 32, 64, 0, "reference"),
+                                              (1000, 20, 50, 1, "reference"),
+                                              (4097, 8, 5, 1, "reference")])
+def test_grid_path_bit_identical(N, k, md, ctrl, mode):
+    """The grid-resident kernel (one cooperative launch per step block, a grid
+    barrier per step) gives bitwise the results of the per-step kernel, for
+    every eligible rows-per-CTA choice, zero delays included."""
+    net = make_network(N, k, 0.1, md, seed=N + md + 3, delay_lo=min(1, md))
+    b = LeviathanEngine(*net.engine_args(), params=dict(gain_controller=ctrl), math_mode=mode)
+    b.set_cluster_mode(False)
+    b.set_grid_mode(False)
+    rb = np.concatenate([b.step_n(DT, 5), b.step_n(DT, 300)])
+    want = _full_state(b)
+    rb_next = b.step(DT)
+    b.close()
+    probe = LeviathanEngine(*net.engine_args(), math_mode=mode)
+    info = probe.grid_info()
+    probe.close()
+    assert info["eligible"] and info["eligible_rows"], info
+    for R in info["eligible_rows"]:
+        a = LeviathanEngine(*net.engine_args(), params=dict(gain_controller=ctrl),
+                            math_mode=mode)
+        a.set_cluster_mode(False)
+        a.set_grid_mode(True, R)
+        assert a.grid_info()["rows_per_cta"] == R
+        ra = np.concatenate([a.step_n(DT, 5), a.step_n(DT, 300)])
+        np.testing.assert_array_equal(ra, rb, err_msg=f"R={R}")
+        got = _full_state(a)
+        for key, w in want.items():
+            np.testing.assert_array_equal(got[key], w, err_msg=f"R={R}: {key}")
+        assert a.step(DT) == rb_next
+        a.close()
+
+
+def test_grid_path_not_used_when_too_large():
+    net = make_network(200_000, 8, 0.1, 8, seed=2)
+    e = LeviathanEngine(*net.engine_args())
+    assert not e.grid_info()["eligible"]
+    e.close()
 
 
 def test_cluster_path_not_used_when_too_large():
@@ -362,6 +416,7 @@ def test_two_steps_per_launch_bit_identical(mode):
                                      math_mode=mode)):
         ref = make()
         ref.set_cluster_mode(False)
+        ref.set_grid_mode(False)
         ref.set_pair_mode(False)
         assert not any(c["enabled"] for c in ref.pair_info())
         r_ref = np.concatenate([ref.step_n(DT, 3), ref.step_n(DT, 64), ref.step_n(DT, 13)])
@@ -370,6 +425,7 @@ def test_two_steps_per_launch_bit_identical(mode):
         for v in range(nvar):
             e = make()
             e.set_cluster_mode(False)
+            e.set_grid_mode(False)
             for c in range(3):
                 e.set_pair_variant(c, v)
             info = e.pair_info()
@@ -391,6 +447,7 @@ def test_zero_delay_takes_one_step_per_launch():
     a = LeviathanEngine(*net.engine_args())
     b = LeviathanEngine(*net.engine_args())
     a.set_cluster_mode(False)
+    a.set_grid_mode(False)
     info = a.pair_info()
     assert not info[0]["eligible"] and not info[0]["enabled"]
     ra = a.step_n(DT, 41)
