@@ -347,6 +347,20 @@ int lev_adj_set_reservoir_grads(LevAdjoint *a, const float *dLdy,
                                 float *grad_win, float *grad_ra,
                                 float *grad_rb);
 
+/* Grid-resident segments (no reference counterpart): for a single network
+ * whose CTAs (64, 128 or 256 rows, four lanes per row) can all be resident
+ * at once, each checkpoint segment is one cooperative launch forward (with
+ * the recording of the backward recompute) and one backward, with a bounded
+ * grid barrier per step; a timeout makes lev_adj_forward / lev_adj_backward
+ * return LEV_ERR_CUDA.  Not used with the reservoir readout (ra, rb).  The
+ * forward trajectory is bitwise that of the per-step kernels; gradients
+ * agree to rounding (sums over a row's edges and over CTAs in another
+ * order).  lev_adj_set_grid_mode: enabled 0 forces per-step launches;
+ * rows_per_cta 0 keeps the current choice. */
+int lev_adj_grid_info(const LevAdjoint *a, int32_t *eligible, int32_t *enabled,
+                      int32_t *rows_per_cta, int32_t *eligible_rows_mask);
+int lev_adj_set_grid_mode(LevAdjoint *a, int32_t enabled, int32_t rows_per_cta);
+
 /* Self-test of the phase wraps (no reference counterpart; checks this
  * library's division-free evaluation of the wraps of
  * leviathan_kernel.cu:105,146,188).  Runs, on the current device, both

@@ -62,6 +62,18 @@ class Adjoint:
         except Exception:
             pass
 
+    def grid_info(self) -> dict:
+        """Whether checkpoint segments run as grid-resident launches (single
+        networks whose CTAs fit on the device at once)."""
+        el, en, r, m = (C.c_int32() for _ in range(4))
+        check(self.lib.lev_adj_grid_info(self._h, C.byref(el), C.byref(en), C.byref(r),
+                                         C.byref(m)))
+        return dict(eligible=bool(el.value), enabled=bool(en.value), rows_per_cta=r.value,
+                    eligible_rows=[R for R in (64, 128, 256) if m.value & R])
+
+    def set_grid_mode(self, enabled: bool, rows_per_cta: int = 0) -> None:
+        check(self.lib.lev_adj_set_grid_mode(self._h, 1 if enabled else 0, int(rows_per_cta)))
+
     @property
     def device_bytes(self) -> int:
         b = C.c_size_t()

@@ -2286,6 +2286,7 @@ LevEngine *leviathan_engine(LeviathanHandle *handle) {
 // lev_adjoint.cuh.
 // ===========================================================================
 #include "lev_adjoint.cuh"
+#include "lev_adj_grid.cuh"
 #include "lev_graphgen.cuh"
 
 namespace lev {
@@ -2474,6 +2475,18 @@ struct LevAdjoint {
   const float *res_dLdy = nullptr;
   float *res_gwin = nullptr, *res_gra = nullptr, *res_grb = nullptr;
   float *ro_partials = nullptr;
+  // grid-resident segments (lev_adj_grid.cuh), single networks only
+  bool grid_ok = false;
+  bool use_grid = true;
+  int grid_R = 0;
+  bool gR_ok[3] = {false, false, false};  // R = 64, 128, 256
+  int g_cap[3] = {0, 0, 0};
+  size_t gf_smem[3] = {0, 0, 0}, gb_smem[3] = {0, 0, 0};
+  int g_nwarps = 0, g_gpad = 0;
+  float2 *g_wsum = nullptr;
+  float *g_lgp = nullptr;
+  unsigned *g_bar = nullptr;
+  int *h_gerr = nullptr, *d_gerr = nullptr;
 };
 
 namespace {
@@ -2501,6 +2514,7 @@ void adj_free(LevAdjoint *a) {
   }
   if (a->ev_start) cudaEventDestroy(a->ev_start);
   if (a->rstream) cudaStreamDestroy(a->rstream);
+  if (a->h_gerr) cudaFreeHost(a->h_gerr);
   delete a;
 }
 
@@ -2577,6 +2591,187 @@ int adj_ckpt(LevAdjoint *a, int seg, bool save, cudaStream_t s = nullptr,
                                        a->ck_g + (size_t)seg * a->NN, nullptr, a->NN);
   }
   LEV_TRY_CUDA(cudaGetLastError());
+  return LEV_OK;
+}
+
+using AdjGridFwdFn = void (*)(AdjGridFwdArgs);
+using AdjGridBwdFn = void (*)(AdjGridBwdArgs);
+AdjGridFwdFn adj_grid_fwd_fn(int R, int math_mode) {
+  const bool acc = math_mode == LEV_MATH_ACCURATE;
+  if (R == 64) return acc ? adj_grid_fwd_kernel<1, 64, 8> : adj_grid_fwd_kernel<0, 64, 8>;
+  if (R == 128) return acc ? adj_grid_fwd_kernel<1, 128, 8> : adj_grid_fwd_kernel<0, 128, 8>;
+  return acc ? adj_grid_fwd_kernel<1, 256, 8> : adj_grid_fwd_kernel<0, 256, 8>;
+}
+AdjGridBwdFn adj_grid_bwd_fn(int R, int math_mode) {
+  const bool acc = math_mode == LEV_MATH_ACCURATE;
+  if (R == 64) return acc ? adj_grid_bwd_kernel<1, 64, 4> : adj_grid_bwd_kernel<0, 64, 4>;
+  if (R == 128) return acc ? adj_grid_bwd_kernel<1, 128, 4> : adj_grid_bwd_kernel<0, 128, 4>;
+  return acc ? adj_grid_bwd_kernel<1, 256, 4> : adj_grid_bwd_kernel<0, 256, 4>;
+}
+
+// Grid-resident segments for a single network: per rows-per-CTA choice, the
+// shared memory of both kernels and whether every CTA can be resident at once.
+int adj_setup_grid(LevAdjoint *a, const std::vector<long long> &sl_off,
+                   const std::vector<int> &sl_len) {
+  a->grid_ok = false;
+  if (a->NN != 1) return LEV_OK;
+  const NetDesc &d = a->h_nets[0];
+  int dev = 0, max_smem = 0, coop = 0, sms = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess ||
+      cudaDeviceGetAttribute(&max_smem, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev) !=
+          cudaSuccess ||
+      cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, dev) != cudaSuccess ||
+      cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess) {
+    cudaGetLastError();
+    return LEV_OK;
+  }
+  if (!coop) return LEV_OK;
+  const int nwarps = 8 * ((d.N + kTile - 1) / kTile);
+  int max_gpad = 0;
+  for (int ri = 0; ri < 3; ++ri) {
+    const int R = kGridRs[ri];
+    const int C = (d.N + R - 1) / R;
+    if (C < 2) continue;
+    const int gpad = (C + 3) & ~3;
+    long long cap = 0;
+    for (int c = 0; c < C; ++c) {
+      long long e = 0;
+      for (int s = c * R / 32; s < std::min<long long>((c + 1) * R / 32, (d.N + 31) / 32); ++s)
+        e += 32LL * sl_len[d.slice_base + s];
+      cap = std::max(cap, e);
+    }
+    const size_t fsm = sizeof(float2) * nwarps + sizeof(float) * 6 * R +
+                       sizeof(int) * 2 * (R / 32) + 8 * (size_t)cap;
+    const size_t bsm = sizeof(float) * (4 * R + gpad) + sizeof(int) * 2 * (R / 32) +
+                       8 * (size_t)cap;
+    if (std::max(fsm, bsm) + 1024 > (size_t)max_smem) continue;
+    bool ok = true;
+    for (int m = 0; m < 2 && ok; ++m) {
+      const int mm = m ? LEV_MATH_ACCURATE : LEV_MATH_REFERENCE;
+      const void *ff = reinterpret_cast<const void *>(adj_grid_fwd_fn(R, mm));
+      const void *bf = reinterpret_cast<const void *>(adj_grid_bwd_fn(R, mm));
+      int pf = 0, pb = 0;
+      ok = cudaFuncSetAttribute(ff, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)fsm) ==
+               cudaSuccess &&
+           cudaFuncSetAttribute(bf, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bsm) ==
+               cudaSuccess &&
+           cudaOccupancyMaxActiveBlocksPerMultiprocessor(&pf, ff, kGridLPR * R, fsm) ==
+               cudaSuccess &&
+           cudaOccupancyMaxActiveBlocksPerMultiprocessor(&pb, bf, kGridLPR * R, bsm) ==
+               cudaSuccess &&
+           (long long)pf * sms >= C && (long long)pb * sms >= C;
+    }
+    cudaGetLastError();
+    if (!ok) continue;
+    a->gR_ok[ri] = true;
+    a->g_cap[ri] = (int)cap;
+    a->gf_smem[ri] = fsm;
+    a->gb_smem[ri] = bsm;
+    max_gpad = std::max(max_gpad, gpad);
+    if (!a->grid_ok) a->grid_R = R;  // the smallest: the most SMs
+    a->grid_ok = true;
+  }
+  if (!a->grid_ok) return LEV_OK;
+  a->g_nwarps = nwarps;
+  a->g_gpad = max_gpad;
+  int rc = adj_alloc(a, &a->g_wsum, 2LL * nwarps);
+  if (rc == LEV_OK) rc = adj_alloc(a, &a->g_lgp, 2LL * max_gpad);
+  if (rc == LEV_OK) rc = adj_alloc(a, &a->g_bar, 1);
+  if (rc != LEV_OK) return rc;
+  LEV_TRY_CUDA(cudaMemset(a->g_wsum, 0, sizeof(float2) * 2 * (size_t)nwarps));
+  LEV_TRY_CUDA(cudaHostAlloc(reinterpret_cast<void **>(&a->h_gerr), sizeof(int),
+                             cudaHostAllocMapped));
+  *a->h_gerr = 0;
+  LEV_TRY_CUDA(cudaHostGetDevicePointer(reinterpret_cast<void **>(&a->d_gerr), a->h_gerr, 0));
+  return LEV_OK;
+}
+
+inline bool adj_grid_on(const LevAdjoint *a) {
+  return a->grid_ok && a->use_grid && a->res_ra == nullptr;
+}
+
+int adj_grid_check(LevAdjoint *a) {
+  if (a->h_gerr && *reinterpret_cast<volatile int *>(a->h_gerr)) {
+    *a->h_gerr = 0;
+    a->grid_ok = false;
+    return fail(LEV_ERR_CUDA,
+                "grid-resident adjoint segment: a grid barrier wait timed out; results are "
+                "undefined");
+  }
+  return LEV_OK;
+}
+
+// One cooperative launch of the grid-resident forward over `n` steps (the
+// per-step record pointers of f start at the segment's first step).
+int adj_grid_launch_fwd(LevAdjoint *a, AdjGridFwdArgs f, int n, cudaStream_t s) {
+  LevEngine *e = a->e;
+  const int R = a->grid_R, ri = grid_r_index(R);
+  LEV_TRY_CUDA(cudaMemsetAsync(a->g_bar, 0, sizeof(unsigned), s));
+  f.net = a->d_nets;
+  f.st = a->d_st;
+  f.row_ptr = e->d_row_ptr;
+  f.sl_off = e->d_sl_off;
+  f.sl_len = e->d_sl_len;
+  f.sl_cd = e->d_sl_cd;
+  f.theta = a->theta;
+  f.theta_hat = a->theta_hat;
+  f.omega = a->omega;
+  f.omega_hat = a->omega_hat;
+  f.wsum = a->g_wsum;
+  f.bar = a->g_bar;
+  f.err = a->d_gerr;
+  f.SL = a->SL;
+  f.early = e->pair_ok ? 1 : 0;  // no delay is 0
+  f.nwarps = a->g_nwarps;
+  f.edge_cap = a->g_cap[ri];
+  f.n_steps = n;
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3((a->h_nets[0].N + R - 1) / R);
+  cfg.blockDim = dim3(kGridLPR * R);
+  cfg.dynamicSmemBytes = a->gf_smem[ri];
+  cfg.stream = s;
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeCooperative;
+  attr[0].val.cooperative = 1;
+  cfg.attrs = attr;
+  cfg.numAttrs = 1;
+  LEV_TRY_CUDA(cudaLaunchKernelEx(&cfg, adj_grid_fwd_fn(R, e->math_mode), f));
+  return LEV_OK;
+}
+
+// One cooperative launch of the grid-resident reverse over the steps of b.
+int adj_grid_launch_bwd(LevAdjoint *a, AdjGridBwdArgs b, cudaStream_t s) {
+  LevEngine *e = a->e;
+  const int R = a->grid_R, ri = grid_r_index(R);
+  LEV_TRY_CUDA(cudaMemsetAsync(a->g_bar, 0, sizeof(unsigned), s));
+  b.net = a->d_nets;
+  b.row_ptr = e->d_row_ptr;
+  b.sl_off = e->d_sl_off;
+  b.sl_len = e->d_sl_len;
+  b.sl_cd = e->d_sl_cd;
+  b.lam_th = a->lam_th;
+  b.lam_thh = a->lam_thh;
+  b.lam_omh = a->lam_omh;
+  b.lam_w = a->lam_w;
+  b.adj_ring = a->adj_ring;
+  b.lam_g = a->lam_g;
+  b.grad_omega = a->grad_omega_acc;
+  b.lgp = a->g_lgp;
+  b.bar = a->g_bar;
+  b.err = a->d_gerr;
+  b.SL = a->SL;
+  b.edge_cap = a->g_cap[ri];
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3((a->h_nets[0].N + R - 1) / R);
+  cfg.blockDim = dim3(kGridLPR * R);
+  cfg.dynamicSmemBytes = a->gb_smem[ri];
+  cfg.stream = s;
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeCooperative;
+  attr[0].val.cooperative = 1;
+  cfg.attrs = attr;
+  cfg.numAttrs = 1;
+  LEV_TRY_CUDA(cudaLaunchKernelEx(&cfg, adj_grid_bwd_fn(R, e->math_mode), b));
   return LEV_OK;
 }
 
@@ -2666,6 +2861,17 @@ int lev_adj_create(LevAdjoint **out, LevEngine *e, int32_t segment,
     }
   }
 #undef A
+  if (rc == LEV_OK && NN == 1) {
+    std::vector<long long> h_off(e->num_slices);
+    std::vector<int> h_len(e->num_slices);
+    if (cudaMemcpy(h_off.data(), e->d_sl_off, sizeof(long long) * e->num_slices,
+                   cudaMemcpyDeviceToHost) != cudaSuccess ||
+        cudaMemcpy(h_len.data(), e->d_sl_len, sizeof(int) * e->num_slices,
+                   cudaMemcpyDeviceToHost) != cudaSuccess)
+      rc = fail(LEV_ERR_CUDA, "adjoint: reading the SELL slice table failed");
+    else
+      rc = adj_setup_grid(a, h_off, h_len);
+  }
   if (rc != LEV_OK) {
     std::string msg = g_last_error;
     adj_free(a);
@@ -2741,6 +2947,36 @@ int lev_adj_forward(LevAdjoint *a, float dt, int32_t T, const float *omega,
   }
   adj_state_kernel<<<1, 128, 0, s>>>(0, a->d_nets, a->d_st, nullptr, K, a->NN);
   LEV_TRY_CUDA(cudaGetLastError());
+  if (adj_grid_on(a)) {
+    // one cooperative launch per checkpoint segment
+    for (int t0 = 0; t0 < T; t0 += a->C) {
+      const int n = std::min(a->C, T - t0);
+      int rc = adj_ckpt(a, t0 / a->C, true);
+      if (rc != LEV_OK) return rc;
+      AdjGridFwdArgs g;
+      std::memset(&g, 0, sizeof(g));
+      g.w_in = a->w;
+      g.w_out = a->w;
+      g.ring = a->ring;
+      g.drive = drive ? drive + (size_t)t0 * a->TN : nullptr;
+      if (a->res_win) {
+        g.win = a->res_win;
+        g.xin = a->res_x + (size_t)t0 * a->NN;
+      }
+      g.r_out = r_out + (size_t)t0 * a->NN;
+      g.theta_out = theta_out ? theta_out + (size_t)t0 * a->TN : nullptr;
+      g.dt = dt;
+      rc = adj_grid_launch_fwd(a, g, n, s);
+      if (rc != LEV_OK) return rc;
+    }
+    LEV_TRY_CUDA(cudaStreamSynchronize(s));
+    int rc = adj_grid_check(a);
+    if (rc != LEV_OK) return rc;
+    a->last_T = T;
+    a->last_dt = dt;
+    a->drive = drive;
+    return LEV_OK;
+  }
   AdjFwdArgs f = adj_fwd_args(a, dt);
   f.drive = nullptr;
   for (int t = 0; t < T; ++t) {
@@ -2796,6 +3032,51 @@ int lev_adj_backward(LevAdjoint *a, const float *dLdr, const float *dLdtheta,
   if (a->res_grb) LEV_TRY_CUDA(cudaMemsetAsync(a->res_grb, 0, nb, s));
   const int nseg = (T + a->C - 1) / a->C;
   const int mode = (e->math_mode == LEV_MATH_ACCURATE) ? 1 : 0;
+  if (adj_grid_on(a)) {
+    // per segment, last to first: restore, recompute (one cooperative
+    // launch, recording), reverse (one cooperative launch)
+    for (int seg = nseg - 1; seg >= 0; --seg) {
+      const int s0 = seg * a->C, n = std::min(T, s0 + a->C) - s0;
+      int rc = adj_ckpt(a, seg, false, s, a->ring);
+      if (rc != LEV_OK) return rc;
+      LEV_TRY_CUDA(cudaMemcpyAsync(a->w_hist, a->w, wb, cudaMemcpyDeviceToDevice, s));
+      AdjGridFwdArgs g;
+      std::memset(&g, 0, sizeof(g));
+      g.w_in = a->w_hist;
+      g.w_rec = a->w_hist + a->SL;
+      g.w_out = a->w_hist + (size_t)n * a->SL;
+      g.ring = a->ring;
+      g.drive = a->drive ? a->drive + (size_t)s0 * a->TN : nullptr;
+      if (a->res_win) {
+        g.win = a->res_win;
+        g.xin = a->res_x + (size_t)s0 * a->NN;
+      }
+      g.thh_rec = a->thh_hist;
+      g.trace = a->trace;
+      g.dt = dt;
+      rc = adj_grid_launch_fwd(a, g, n, s);
+      if (rc != LEV_OK) return rc;
+      AdjGridBwdArgs b;
+      std::memset(&b, 0, sizeof(b));
+      b.w_hist = a->w_hist;
+      b.H = a->ring;
+      b.thh_hist = a->thh_hist;
+      b.trace = a->trace;
+      b.dLdr = dLdr;
+      b.dLdth = dLdtheta;
+      b.grad_drive = grad_drive;
+      if (a->res_win) {
+        b.win = a->res_win;
+        b.xin = a->res_x;
+        b.grad_win = a->res_gwin;
+      }
+      b.seg_start = s0;
+      b.n_steps = n;
+      b.dt = dt;
+      rc = adj_grid_launch_bwd(a, b, s);
+      if (rc != LEV_OK) return rc;
+    }
+  } else {
   // Segment k-1 is recomputed (stream rs, record set (k-1)&1) while segment k
   // is reversed (engine stream, record set k&1), when the second set exists.
   const bool overlap = a->rstream != nullptr && nseg > 1;
@@ -2914,6 +3195,7 @@ int lev_adj_backward(LevAdjoint *a, const float *dLdr, const float *dLdtheta,
       if (rc != LEV_OK) return rc;
     }
   }
+  }  // per-step launches
   // gradients
   dim3 grid(64, a->NN);
   adj_finalize_kernel<<<grid, 256, 0, s>>>(a->d_nets, a->NN, a->lam_th, a->adj_ring,
@@ -2938,6 +3220,34 @@ int lev_adj_backward(LevAdjoint *a, const float *dLdr, const float *dLdtheta,
                                  cudaMemcpyDeviceToDevice, s));
   LEV_TRY_CUDA(cudaGetLastError());
   LEV_TRY_CUDA(cudaStreamSynchronize(s));
+  return adj_grid_check(a);
+}
+
+int lev_adj_grid_info(const LevAdjoint *a, int32_t *eligible, int32_t *enabled,
+                      int32_t *rows_per_cta, int32_t *eligible_rows_mask) {
+  if (!a) return fail(LEV_ERR_ARG, "null handle");
+  if (eligible) *eligible = a->grid_ok ? 1 : 0;
+  if (enabled) *enabled = adj_grid_on(a) ? 1 : 0;
+  if (rows_per_cta) *rows_per_cta = a->grid_ok ? a->grid_R : 0;
+  if (eligible_rows_mask) {
+    int m = 0;
+    for (int i = 0; i < 3; ++i)
+      if (a->gR_ok[i]) m |= kGridRs[i];
+    *eligible_rows_mask = m;
+  }
+  return LEV_OK;
+}
+
+int lev_adj_set_grid_mode(LevAdjoint *a, int32_t enabled, int32_t rows_per_cta) {
+  if (!a) return fail(LEV_ERR_ARG, "null handle");
+  if (rows_per_cta != 0) {
+    if (rows_per_cta != 64 && rows_per_cta != 128 && rows_per_cta != 256)
+      return fail(LEV_ERR_ARG, "rows_per_cta must be 0, 64, 128 or 256");
+    if (!a->gR_ok[grid_r_index(rows_per_cta)])
+      return fail(LEV_ERR_ARG, "rows_per_cta not eligible for this adjoint");
+    a->grid_R = rows_per_cta;
+  }
+  a->use_grid = enabled != 0;
   return LEV_OK;
 }
 
