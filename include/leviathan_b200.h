@@ -356,10 +356,15 @@ int lev_adj_set_reservoir_grads(LevAdjoint *a, const float *dLdy,
  * forward trajectory is bitwise that of the per-step kernels; gradients
  * agree to rounding (sums over a row's edges and over CTAs in another
  * order).  lev_adj_set_grid_mode: enabled 0 forces per-step launches;
- * rows_per_cta 0 keeps the current choice. */
+ * rows_per_cta 0 keeps the current choice.  When a second segment record set
+ * fits and both CTA groups fit on the device at once, the backward pass
+ * recomputes segment k-1 and reverses segment k in ONE paired launch (two
+ * CTA groups, one barrier counter each); *paired tells whether it does;
+ * lev_adj_set_grid_pairing(a, 0) makes the two separate launches again. */
 int lev_adj_grid_info(const LevAdjoint *a, int32_t *eligible, int32_t *enabled,
-                      int32_t *rows_per_cta, int32_t *eligible_rows_mask);
+                      int32_t *rows_per_cta, int32_t *eligible_rows_mask, int32_t *paired);
 int lev_adj_set_grid_mode(LevAdjoint *a, int32_t enabled, int32_t rows_per_cta);
+int lev_adj_set_grid_pairing(LevAdjoint *a, int32_t enabled);
 
 /* Self-test of the phase wraps (no reference counterpart; checks this
  * library's division-free evaluation of the wraps of

@@ -129,8 +129,9 @@ PROTOTYPES = {
     "lev_adj_set_reservoir": (C.c_int, [_P, _P, _P, _P, _P, _P]),
     "lev_adj_set_reservoir_grads": (C.c_int, [_P, _P, _P, _P, _P]),
     "lev_adj_grid_info": (C.c_int, [_P, C.POINTER(_i32), C.POINTER(_i32), C.POINTER(_i32),
-                                    C.POINTER(_i32)]),
+                                    C.POINTER(_i32), C.POINTER(_i32)]),
     "lev_adj_set_grid_mode": (C.c_int, [_P, _i32, _i32]),
+    "lev_adj_set_grid_pairing": (C.c_int, [_P, _i32]),
     "lev_selftest_wraps":(C.c_int, [C.POINTER(C.c_uint64), C.POINTER(C.c_uint64)]),
     "lev_step_noalloc":(C.c_int, [_i32, _i32, _i64, _P, _P, _P, _P, _P, _P, _P,
                                    _P, _P, _P, _P, C.POINTER(LevParams), _f32,

@@ -65,14 +65,20 @@ class Adjoint:
     def grid_info(self) -> dict:
         """Whether checkpoint segments run as grid-resident launches (single
         networks whose CTAs fit on the device at once)."""
-        el, en, r, m = (C.c_int32() for _ in range(4))
+        el, en, r, m, pr = (C.c_int32() for _ in range(5))
         check(self.lib.lev_adj_grid_info(self._h, C.byref(el), C.byref(en), C.byref(r),
-                                         C.byref(m)))
+                                         C.byref(m), C.byref(pr)))
         return dict(eligible=bool(el.value), enabled=bool(en.value), rows_per_cta=r.value,
-                    eligible_rows=[R for R in (64, 128, 256) if m.value & R])
+                    eligible_rows=[R for R in (64, 128, 256) if m.value & R],
+                    paired=bool(pr.value))
 
     def set_grid_mode(self, enabled: bool, rows_per_cta: int = 0) -> None:
         check(self.lib.lev_adj_set_grid_mode(self._h, 1 if enabled else 0, int(rows_per_cta)))
+
+    def set_grid_pairing(self, enabled: bool) -> None:
+        """Recompute segment k-1 and reverse segment k in one paired launch
+        (when eligible), or in launches of their own."""
+        check(self.lib.lev_adj_set_grid_pairing(self._h, 1 if enabled else 0))
 
     @property
     def device_bytes(self) -> int:

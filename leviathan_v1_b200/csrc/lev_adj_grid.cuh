@@ -19,7 +19,12 @@
 //                        dt S_i: every CTA writes its part, and after the grid
 //                        barrier every CTA adds the parts in the same order.
 //                        One barrier per reverse step orders the scatters into
-//                        slot s+1 before reverse step s reads it.
+//                        slot s+1 before reverse step s reads it.  Only lam_g
+//                        needs the barrier of the step reversed just before:
+//                        the history, weight and trace loads of step s, the
+//                        first group of its edge loads and, without zero
+//                        delays, its adjoint-ring slot (whose scatters came
+//                        from steps s+2 and later) are issued before the wait.
 // Both use the bounded barrier of lev_grid.cuh (error flag on a timeout).
 
 #pragma once
@@ -62,17 +67,17 @@ struct AdjGridFwdArgs {
 // R rows per CTA, four lanes per row; U edges per lane in flight together.
 // Shared memory: s_ws float2[nwarps], th/thh/om/omh float[R], ord float[2R],
 // sloff/sllen int[R/32], cd uint32[edge_cap], w float[edge_cap].
+// The body runs as CTA `cta` of a group of G CTAs (the whole grid, or one
+// half of a paired launch).
 template <int MATH, int R, int U>
-__global__ void __launch_bounds__(kGridLPR * R, 256 / R)
-    adj_grid_fwd_kernel(const AdjGridFwdArgs a) {
+__device__ __forceinline__ void adj_grid_fwd_body(const AdjGridFwdArgs &a, const int cta,
+                                                  const unsigned G, unsigned char *smem) {
   constexpr int LPR = kGridLPR;
   constexpr int nslices = R / 32;
-  extern __shared__ __align__(16) unsigned char smem[];
   __shared__ float s_g;
   __shared__ int s_ok;
 
   const NetDesc nd = *a.net;
-  const int cta = blockIdx.x;
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   const int q = tid & (LPR - 1);
   const int rloc = tid / LPR;
@@ -137,7 +142,6 @@ __global__ void __launch_bounds__(kGridLPR * R, 256 / R)
   const float w_min = nd.w_min, w_max = nd.w_max;
   const int wslice = (warp * (32 / LPR)) / 32;
   const bool slice_live = row0 + wslice * 32 < N;
-  const unsigned G = gridDim.x;
   if (tid == 0) s_ok = 1;
   __syncthreads();
 
@@ -342,9 +346,10 @@ struct AdjGridBwdArgs {
   float *adj_ring;
   float *lam_g;          // [1]: in lam_g(seg_end), out lam_g(seg_start)
   float *grad_omega;     // accumulated
-  float *lgp;            // [2][gridDim.x rounded up to 4] per-CTA lam_g parts
+  float *lgp;            // [2][group CTAs rounded up to 4] per-CTA lam_g parts
   unsigned *bar;
   int *err;
+  int early;             // no delay is 0: slot s+1 is complete one barrier earlier
   long long SL;
   long long seg_start;
   int n_steps;           // reverse steps seg_start + n_steps - 1 .. seg_start
@@ -356,18 +361,15 @@ struct AdjGridBwdArgs {
 // Shared memory: lt/lthh/lomh/go float[R], lgp float[G rounded up to 4],
 // sloff/sllen int[R/32], cd uint32[edge_cap], lw float[edge_cap].
 template <int MATH, int R, int U>
-__global__ void __launch_bounds__(kGridLPR * R, 256 / R)
-    adj_grid_bwd_kernel(const AdjGridBwdArgs a) {
+__device__ __forceinline__ void adj_grid_bwd_body(const AdjGridBwdArgs &a, const int cta,
+                                                  const unsigned G, unsigned char *smem) {
   constexpr int LPR = kGridLPR;
   constexpr int nslices = R / 32;
-  extern __shared__ __align__(16) unsigned char smem[];
   __shared__ float s_red[32];
   __shared__ float s_lg;
   __shared__ int s_ok;
 
   const NetDesc nd = *a.net;
-  const int cta = blockIdx.x;
-  const unsigned G = gridDim.x;
   const int gpad = ((int)G + 3) & ~3;
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   const int q = tid & (LPR - 1);
@@ -470,13 +472,43 @@ __global__ void __launch_bounds__(kGridLPR * R, 256 / R)
       dgdg = free ? 1.0f - dt * nd.mu : 0.0f;
     }
     const float Cm = tr.z * invN, Sm = tr.w * invN;
-    float th = 0.0f, eps = 0.0f, diff = 0.0f, th1 = 0.0f;
+    float th = 0.0f, eps = 0.0f, diff = 0.0f, sn1 = 0.0f, cs1 = 0.0f, arv = 0.0f;
+    float *slot_next = AR + (long long)as_next * Np + row;
     if (live) {
       th = H[(long long)hs * Np + row];
       diff = wrap_pm_pi(th - a.thh_hist[(long long)kk * N + gi]);
       eps = sinf(diff);
-      if (q == 0) th1 = H[(long long)(hs + 1) * Np + row];
+      if (q == 0) {
+        sincosf(H[(long long)(hs + 1) * Np + row], &sn1, &cs1);
+        if (a.early) {
+          arv = __ldcg(slot_next);
+          __stcg(slot_next, 0.0f);
+        }
+      }
     }
+    // first group of edge loads (nothing in them depends on lam)
+    const int len = slice_live ? sllen[wslice] : 0;
+    const int base = sloff[wslice] + (rloc & 31);
+    const float *w_s = a.w_hist + (long long)kk * a.SL + ebase;
+    uint32_t p[U];
+    float wv[U], lw[U], dj[U];
+    auto load_group = [&](int kb) {
+#pragma unroll
+      for (int u = 0; u < U; ++u) {
+        const int e = kb + LPR * u + q;
+        const bool in = e < deg;
+        p[u] = in ? s_cd[base + 32 * e] : 0u;
+        wv[u] = in ? __ldg(w_s + base + 32 * e) : 0.0f;
+        lw[u] = in ? s_lw[base + 32 * e] : 0.0f;
+      }
+#pragma unroll
+      for (int u = 0; u < U; ++u) {
+        const int d = (int)(p[u] & 255u);
+        dj[u] = __ldg(H + (long long)(hs - d) * Np + (p[u] >> 8));
+      }
+    };
+    if (len > 0) load_group(0);
+    const float dldr = a.dLdr ? a.dLdr[s] : 0.0f;
     // lam_g(s+1): the parts of reverse step s+1, after its barrier
     if (k > 0) {
       if (!(ok = grid_wait(a.bar, (unsigned)k * G, a.err, &s_ok))) break;
@@ -485,16 +517,16 @@ __global__ void __launch_bounds__(kGridLPR * R, 256 / R)
       lamg = s_lg;
     }
     dgdg_prev = dgdg;
-    const float lam_r = (a.dLdr ? a.dLdr[s] : 0.0f) + lamg * dgdr;
+    const float lam_r = dldr + lamg * dgdr;
     float lt1 = 0.0f;
     if (live && q == 0) {
       // (A) adjoint of theta(s+1), complete; (B) integrate
-      float *slot_next = AR + (long long)as_next * Np + row;
-      lt1 = s_lt[rloc] + __ldcg(slot_next);
-      __stcg(slot_next, 0.0f);
-      float sn, cs;
-      sincosf(th1, &sn, &cs);
-      if (r1 > 0.0f) lt1 += lam_r * (Sm * cs - Cm * sn) * invN / r1;
+      if (!a.early) {
+        arv = __ldcg(slot_next);
+        __stcg(slot_next, 0.0f);
+      }
+      lt1 = s_lt[rloc] + arv;
+      if (r1 > 0.0f) lt1 += lam_r * (Sm * cs1 - Cm * sn1) * invN / r1;
       if (a.dLdth) lt1 += a.dLdth[s * N + gi];
       s_go[rloc] += lt1 * dt;
       if (a.grad_drive) a.grad_drive[s * N + gi] = lt1 * dt;
@@ -504,48 +536,29 @@ __global__ void __launch_bounds__(kGridLPR * R, 256 / R)
     const float lam_S = lt1 * dt * g_s;
     const float ae = fabsf(eps);
     float S_i = 0.0f, lsum = 0.0f, labs = 0.0f;
-    if (slice_live) {
-      const int len = sllen[wslice];
-      const int base = sloff[wslice] + (rloc & 31);
-      const float *w_s = a.w_hist + (long long)kk * a.SL + ebase;
-      for (int kb = 0; kb < len; kb += LPR * U) {
-        uint32_t p[U];
-        float wv[U], lw[U], dj[U];
+    for (int kb = 0; kb < len; kb += LPR * U) {
+      if (kb > 0) load_group(kb);
 #pragma unroll
-        for (int u = 0; u < U; ++u) {
-          const int e = kb + LPR * u + q;
-          const bool in = e < deg;
-          p[u] = in ? s_cd[base + 32 * e] : 0u;
-          wv[u] = in ? __ldg(w_s + base + 32 * e) : 0.0f;
-          lw[u] = in ? s_lw[base + 32 * e] : 0.0f;
-        }
-#pragma unroll
-        for (int u = 0; u < U; ++u) {
-          const int d = (int)(p[u] & 255u);
-          dj[u] = __ldg(H + (long long)(hs - d) * Np + (p[u] >> 8));
-        }
-#pragma unroll
-        for (int u = 0; u < U; ++u) {
-          const int e = kb + LPR * u + q;
-          if (e < deg) {
-            const int j = (int)(p[u] >> 8), d = (int)(p[u] & 255u);
-            const float delayed_j = dj[u];
-            float dlt = delayed_j - th;
-            dlt = wrap_pm_pi(dlt);
-            const float w = wv[u];
-            float sn, cs;
-            lev_sincos<MATH>(dlt, &sn, &cs);
-            S_i += w * sn;
-            const float w_pre = w + dt * (eta * cs * (1.0f - gamma * ae) - lam * w);
-            const float c = (w_pre >= w_min && w_pre <= w_max) ? 1.0f : 0.0f;
-            const float lwn = lw[u];
-            s_lw[base + 32 * e] = lwn * c * decay + lam_S * sn;
-            const float lD = lam_S * w * cs - lwn * c * dt * eta * sn * (1.0f - gamma * ae);
-            labs -= lwn * c * dt * eta * gamma * cs;
-            const int slot = (as_s - d < 0) ? as_s - d + bsa : as_s - d;
-            atomicAdd(AR + (long long)slot * Np + j, lD);
-            lsum -= lD;
-          }
+      for (int u = 0; u < U; ++u) {
+        const int e = kb + LPR * u + q;
+        if (e < deg) {
+          const int j = (int)(p[u] >> 8), d = (int)(p[u] & 255u);
+          const float delayed_j = dj[u];
+          float dlt = delayed_j - th;
+          dlt = wrap_pm_pi(dlt);
+          const float w = wv[u];
+          float sn, cs;
+          lev_sincos<MATH>(dlt, &sn, &cs);
+          S_i += w * sn;
+          const float w_pre = w + dt * (eta * cs * (1.0f - gamma * ae) - lam * w);
+          const float c = (w_pre >= w_min && w_pre <= w_max) ? 1.0f : 0.0f;
+          const float lwn = lw[u];
+          s_lw[base + 32 * e] = lwn * c * decay + lam_S * sn;
+          const float lD = lam_S * w * cs - lwn * c * dt * eta * sn * (1.0f - gamma * ae);
+          labs -= lwn * c * dt * eta * gamma * cs;
+          const int slot = (as_s - d < 0) ? as_s - d + bsa : as_s - d;
+          atomicAdd(AR + (long long)slot * Np + j, lD);
+          lsum -= lD;
         }
       }
     }
@@ -595,6 +608,35 @@ __global__ void __launch_bounds__(kGridLPR * R, 256 / R)
     a.grad_omega[gi] = s_go[rloc];
   }
   for (int e = tid; e < nent; e += blockDim.x) a.lam_w[ebase + e] = s_lw[e];
+}
+
+template <int MATH, int R, int U>
+__global__ void __launch_bounds__(kGridLPR * R, 256 / R)
+    adj_grid_fwd_kernel(const AdjGridFwdArgs a) {
+  extern __shared__ __align__(16) unsigned char smem[];
+  adj_grid_fwd_body<MATH, R, U>(a, blockIdx.x, gridDim.x, smem);
+}
+
+template <int MATH, int R, int U>
+__global__ void __launch_bounds__(kGridLPR * R, R == 64 ? 2 : 1)
+    adj_grid_bwd_kernel(const AdjGridBwdArgs a) {
+  extern __shared__ __align__(16) unsigned char smem[];
+  adj_grid_bwd_body<MATH, R, U>(a, blockIdx.x, gridDim.x, smem);
+}
+
+// Paired launch of the backward pass: CTAs [0, gf) recompute segment k-1
+// into one record set while CTAs [gf, grid) reverse segment k from the
+// other; each group has its own barrier counter and shares the SMs with the
+// other, so the two latency-bound step chains overlap.  Every CTA of both
+// groups is resident at once (cooperative launch).
+template <int MATH, int R, int UF, int UB>
+__global__ void __launch_bounds__(kGridLPR * R, 256 / R)
+    adj_grid_pair_kernel(const AdjGridFwdArgs f, const AdjGridBwdArgs b, const int gf) {
+  extern __shared__ __align__(16) unsigned char smem[];
+  if ((int)blockIdx.x < gf)
+    adj_grid_fwd_body<MATH, R, UF>(f, blockIdx.x, gf, smem);
+  else
+    adj_grid_bwd_body<MATH, R, UB>(b, blockIdx.x - gf, gridDim.x - gf, smem);
 }
 
 }  // namespace lev

@@ -2482,6 +2482,8 @@ struct LevAdjoint {
   bool gR_ok[3] = {false, false, false};  // R = 64, 128, 256
   int g_cap[3] = {0, 0, 0};
   size_t gf_smem[3] = {0, 0, 0}, gb_smem[3] = {0, 0, 0};
+  bool gp_ok[3] = {false, false, false};  // paired recompute + reverse launch fits
+  bool use_pair = true;
   int g_nwarps = 0, g_gpad = 0;
   float2 *g_wsum = nullptr;
   float *g_lgp = nullptr;
@@ -2602,10 +2604,18 @@ AdjGridFwdFn adj_grid_fwd_fn(int R, int math_mode) {
   if (R == 128) return acc ? adj_grid_fwd_kernel<1, 128, 8> : adj_grid_fwd_kernel<0, 128, 8>;
   return acc ? adj_grid_fwd_kernel<1, 256, 8> : adj_grid_fwd_kernel<0, 256, 8>;
 }
+using AdjGridPairFn = void (*)(AdjGridFwdArgs, AdjGridBwdArgs, int);
+AdjGridPairFn adj_grid_pair_fn(int R, int math_mode) {
+  const bool acc = math_mode == LEV_MATH_ACCURATE;
+  if (R == 64) return acc ? adj_grid_pair_kernel<1, 64, 8, 4> : adj_grid_pair_kernel<0, 64, 8, 4>;
+  if (R == 128)
+    return acc ? adj_grid_pair_kernel<1, 128, 8, 4> : adj_grid_pair_kernel<0, 128, 8, 4>;
+  return acc ? adj_grid_pair_kernel<1, 256, 8, 4> : adj_grid_pair_kernel<0, 256, 8, 4>;
+}
 AdjGridBwdFn adj_grid_bwd_fn(int R, int math_mode) {
   const bool acc = math_mode == LEV_MATH_ACCURATE;
-  if (R == 64) return acc ? adj_grid_bwd_kernel<1, 64, 4> : adj_grid_bwd_kernel<0, 64, 4>;
-  if (R == 128) return acc ? adj_grid_bwd_kernel<1, 128, 4> : adj_grid_bwd_kernel<0, 128, 4>;
+  if (R == 64) return acc ? adj_grid_bwd_kernel<1, 64, 8> : adj_grid_bwd_kernel<0, 64, 8>;
+  if (R == 128) return acc ? adj_grid_bwd_kernel<1, 128, 8> : adj_grid_bwd_kernel<0, 128, 8>;
   return acc ? adj_grid_bwd_kernel<1, 256, 4> : adj_grid_bwd_kernel<0, 256, 4>;
 }
 
@@ -2663,6 +2673,21 @@ int adj_setup_grid(LevAdjoint *a, const std::vector<long long> &sl_off,
     }
     cudaGetLastError();
     if (!ok) continue;
+    // the paired backward launch: both groups resident at once
+    bool pok = true;
+    for (int m = 0; m < 2 && pok; ++m) {
+      const void *pf = reinterpret_cast<const void *>(
+          adj_grid_pair_fn(R, m ? LEV_MATH_ACCURATE : LEV_MATH_REFERENCE));
+      const size_t psm = std::max(fsm, bsm);
+      int per_sm = 0;
+      pok = cudaFuncSetAttribute(pf, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)psm) ==
+                cudaSuccess &&
+            cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, pf, kGridLPR * R, psm) ==
+                cudaSuccess &&
+            (long long)per_sm * sms >= 2LL * C;
+    }
+    cudaGetLastError();
+    a->gp_ok[ri] = pok;
     a->gR_ok[ri] = true;
     a->g_cap[ri] = (int)cap;
     a->gf_smem[ri] = fsm;
@@ -2676,7 +2701,7 @@ int adj_setup_grid(LevAdjoint *a, const std::vector<long long> &sl_off,
   a->g_gpad = max_gpad;
   int rc = adj_alloc(a, &a->g_wsum, 2LL * nwarps);
   if (rc == LEV_OK) rc = adj_alloc(a, &a->g_lgp, 2LL * max_gpad);
-  if (rc == LEV_OK) rc = adj_alloc(a, &a->g_bar, 1);
+  if (rc == LEV_OK) rc = adj_alloc(a, &a->g_bar, 2);
   if (rc != LEV_OK) return rc;
   LEV_TRY_CUDA(cudaMemset(a->g_wsum, 0, sizeof(float2) * 2 * (size_t)nwarps));
   LEV_TRY_CUDA(cudaHostAlloc(reinterpret_cast<void **>(&a->h_gerr), sizeof(int),
@@ -2701,12 +2726,10 @@ int adj_grid_check(LevAdjoint *a) {
   return LEV_OK;
 }
 
-// One cooperative launch of the grid-resident forward over `n` steps (the
-// per-step record pointers of f start at the segment's first step).
-int adj_grid_launch_fwd(LevAdjoint *a, AdjGridFwdArgs f, int n, cudaStream_t s) {
+// The fields of a forward segment that do not depend on the segment.
+void adj_grid_fill_fwd(LevAdjoint *a, AdjGridFwdArgs &f, int n) {
   LevEngine *e = a->e;
-  const int R = a->grid_R, ri = grid_r_index(R);
-  LEV_TRY_CUDA(cudaMemsetAsync(a->g_bar, 0, sizeof(unsigned), s));
+  const int ri = grid_r_index(a->grid_R);
   f.net = a->d_nets;
   f.st = a->d_st;
   f.row_ptr = e->d_row_ptr;
@@ -2725,6 +2748,15 @@ int adj_grid_launch_fwd(LevAdjoint *a, AdjGridFwdArgs f, int n, cudaStream_t s) 
   f.nwarps = a->g_nwarps;
   f.edge_cap = a->g_cap[ri];
   f.n_steps = n;
+}
+
+// One cooperative launch of the grid-resident forward over `n` steps (the
+// per-step record pointers of f start at the segment's first step).
+int adj_grid_launch_fwd(LevAdjoint *a, AdjGridFwdArgs f, int n, cudaStream_t s) {
+  LevEngine *e = a->e;
+  const int R = a->grid_R, ri = grid_r_index(R);
+  LEV_TRY_CUDA(cudaMemsetAsync(a->g_bar, 0, sizeof(unsigned), s));
+  adj_grid_fill_fwd(a, f, n);
   cudaLaunchConfig_t cfg = {};
   cfg.gridDim = dim3((a->h_nets[0].N + R - 1) / R);
   cfg.blockDim = dim3(kGridLPR * R);
@@ -2739,11 +2771,10 @@ int adj_grid_launch_fwd(LevAdjoint *a, AdjGridFwdArgs f, int n, cudaStream_t s) 
   return LEV_OK;
 }
 
-// One cooperative launch of the grid-resident reverse over the steps of b.
-int adj_grid_launch_bwd(LevAdjoint *a, AdjGridBwdArgs b, cudaStream_t s) {
+// The fields of a reverse segment that do not depend on the segment.
+void adj_grid_fill_bwd(LevAdjoint *a, AdjGridBwdArgs &b) {
   LevEngine *e = a->e;
-  const int R = a->grid_R, ri = grid_r_index(R);
-  LEV_TRY_CUDA(cudaMemsetAsync(a->g_bar, 0, sizeof(unsigned), s));
+  const int ri = grid_r_index(a->grid_R);
   b.net = a->d_nets;
   b.row_ptr = e->d_row_ptr;
   b.sl_off = e->d_sl_off;
@@ -2759,8 +2790,17 @@ int adj_grid_launch_bwd(LevAdjoint *a, AdjGridBwdArgs b, cudaStream_t s) {
   b.lgp = a->g_lgp;
   b.bar = a->g_bar;
   b.err = a->d_gerr;
+  b.early = e->pair_ok ? 1 : 0;  // no delay is 0
   b.SL = a->SL;
   b.edge_cap = a->g_cap[ri];
+}
+
+// One cooperative launch of the grid-resident reverse over the steps of b.
+int adj_grid_launch_bwd(LevAdjoint *a, AdjGridBwdArgs b, cudaStream_t s) {
+  LevEngine *e = a->e;
+  const int R = a->grid_R, ri = grid_r_index(R);
+  LEV_TRY_CUDA(cudaMemsetAsync(a->g_bar, 0, sizeof(unsigned), s));
+  adj_grid_fill_bwd(a, b);
   cudaLaunchConfig_t cfg = {};
   cfg.gridDim = dim3((a->h_nets[0].N + R - 1) / R);
   cfg.blockDim = dim3(kGridLPR * R);
@@ -2772,6 +2812,33 @@ int adj_grid_launch_bwd(LevAdjoint *a, AdjGridBwdArgs b, cudaStream_t s) {
   cfg.attrs = attr;
   cfg.numAttrs = 1;
   LEV_TRY_CUDA(cudaLaunchKernelEx(&cfg, adj_grid_bwd_fn(R, e->math_mode), b));
+  return LEV_OK;
+}
+
+// The paired backward launch: the forward segment f (n steps) on CTAs
+// [0, C), the reverse segment b on CTAs [C, 2C), each group with its own
+// barrier counter.
+int adj_grid_launch_pair(LevAdjoint *a, AdjGridFwdArgs f, int n, AdjGridBwdArgs b,
+                         cudaStream_t s) {
+  LevEngine *e = a->e;
+  const int R = a->grid_R, ri = grid_r_index(R);
+  const int C = (a->h_nets[0].N + R - 1) / R;
+  LEV_TRY_CUDA(cudaMemsetAsync(a->g_bar, 0, 2 * sizeof(unsigned), s));
+  adj_grid_fill_fwd(a, f, n);
+  adj_grid_fill_bwd(a, b);
+  f.bar = a->g_bar;
+  b.bar = a->g_bar + 1;
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3(2 * C);
+  cfg.blockDim = dim3(kGridLPR * R);
+  cfg.dynamicSmemBytes = std::max(a->gf_smem[ri], a->gb_smem[ri]);
+  cfg.stream = s;
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeCooperative;
+  attr[0].val.cooperative = 1;
+  cfg.attrs = attr;
+  cfg.numAttrs = 1;
+  LEV_TRY_CUDA(cudaLaunchKernelEx(&cfg, adj_grid_pair_fn(R, e->math_mode), f, b, C));
   return LEV_OK;
 }
 
@@ -3033,35 +3100,45 @@ int lev_adj_backward(LevAdjoint *a, const float *dLdr, const float *dLdtheta,
   const int nseg = (T + a->C - 1) / a->C;
   const int mode = (e->math_mode == LEV_MATH_ACCURATE) ? 1 : 0;
   if (adj_grid_on(a)) {
-    // per segment, last to first: restore, recompute (one cooperative
-    // launch, recording), reverse (one cooperative launch)
-    for (int seg = nseg - 1; seg >= 0; --seg) {
-      const int s0 = seg * a->C, n = std::min(T, s0 + a->C) - s0;
-      int rc = adj_ckpt(a, seg, false, s, a->ring);
+    // Segments last to first.  Segment k's records go to set k & 1 when a
+    // second set exists.  Recompute of segment k-1 and reverse of segment k
+    // share one paired launch when both groups fit on the device; otherwise
+    // each segment is recomputed, then reversed, in launches of their own.
+    const bool two = a->ring2 != nullptr;
+    const bool paired = two && a->use_pair && a->gp_ok[grid_r_index(a->grid_R)] && nseg > 1;
+    float *rings[2] = {a->ring, two ? a->ring2 : a->ring};
+    float *whs[2] = {a->w_hist, two ? a->w_hist2 : a->w_hist};
+    float *ths[2] = {a->thh_hist, two ? a->thh_hist2 : a->thh_hist};
+    float4 *trs[2] = {a->trace, two ? a->trace2 : a->trace};
+    auto seg_len = [&](int seg) { return std::min(T, seg * a->C + a->C) - seg * a->C; };
+    // restore segment `seg` and describe its recompute into its record set
+    auto prep_fwd = [&](int seg, AdjGridFwdArgs &g) -> int {
+      const int s0 = seg * a->C, n = seg_len(seg), k = paired ? (seg & 1) : 0;
+      int rc = adj_ckpt(a, seg, false, s, rings[k]);
       if (rc != LEV_OK) return rc;
-      LEV_TRY_CUDA(cudaMemcpyAsync(a->w_hist, a->w, wb, cudaMemcpyDeviceToDevice, s));
-      AdjGridFwdArgs g;
+      LEV_TRY_CUDA(cudaMemcpyAsync(whs[k], a->w, wb, cudaMemcpyDeviceToDevice, s));
       std::memset(&g, 0, sizeof(g));
-      g.w_in = a->w_hist;
-      g.w_rec = a->w_hist + a->SL;
-      g.w_out = a->w_hist + (size_t)n * a->SL;
-      g.ring = a->ring;
+      g.w_in = whs[k];
+      g.w_rec = whs[k] + a->SL;
+      g.w_out = whs[k] + (size_t)n * a->SL;
+      g.ring = rings[k];
       g.drive = a->drive ? a->drive + (size_t)s0 * a->TN : nullptr;
       if (a->res_win) {
         g.win = a->res_win;
         g.xin = a->res_x + (size_t)s0 * a->NN;
       }
-      g.thh_rec = a->thh_hist;
-      g.trace = a->trace;
+      g.thh_rec = ths[k];
+      g.trace = trs[k];
       g.dt = dt;
-      rc = adj_grid_launch_fwd(a, g, n, s);
-      if (rc != LEV_OK) return rc;
-      AdjGridBwdArgs b;
+      return LEV_OK;
+    };
+    auto prep_bwd = [&](int seg, AdjGridBwdArgs &b) {
+      const int k = paired ? (seg & 1) : 0;
       std::memset(&b, 0, sizeof(b));
-      b.w_hist = a->w_hist;
-      b.H = a->ring;
-      b.thh_hist = a->thh_hist;
-      b.trace = a->trace;
+      b.w_hist = whs[k];
+      b.H = rings[k];
+      b.thh_hist = ths[k];
+      b.trace = trs[k];
       b.dLdr = dLdr;
       b.dLdth = dLdtheta;
       b.grad_drive = grad_drive;
@@ -3070,12 +3147,34 @@ int lev_adj_backward(LevAdjoint *a, const float *dLdr, const float *dLdtheta,
         b.xin = a->res_x;
         b.grad_win = a->res_gwin;
       }
-      b.seg_start = s0;
-      b.n_steps = n;
+      b.seg_start = (long long)seg * a->C;
+      b.n_steps = seg_len(seg);
       b.dt = dt;
-      rc = adj_grid_launch_bwd(a, b, s);
-      if (rc != LEV_OK) return rc;
+    };
+    AdjGridFwdArgs g;
+    AdjGridBwdArgs b;
+    int rc = LEV_OK;
+    if (paired) {
+      rc = prep_fwd(nseg - 1, g);
+      if (rc == LEV_OK) rc = adj_grid_launch_fwd(a, g, seg_len(nseg - 1), s);
+      for (int seg = nseg - 1; seg >= 0 && rc == LEV_OK; --seg) {
+        prep_bwd(seg, b);
+        if (seg > 0) {
+          rc = prep_fwd(seg - 1, g);
+          if (rc == LEV_OK) rc = adj_grid_launch_pair(a, g, seg_len(seg - 1), b, s);
+        } else {
+          rc = adj_grid_launch_bwd(a, b, s);
+        }
+      }
+    } else {
+      for (int seg = nseg - 1; seg >= 0 && rc == LEV_OK; --seg) {
+        rc = prep_fwd(seg, g);
+        if (rc == LEV_OK) rc = adj_grid_launch_fwd(a, g, seg_len(seg), s);
+        prep_bwd(seg, b);
+        if (rc == LEV_OK) rc = adj_grid_launch_bwd(a, b, s);
+      }
     }
+    if (rc != LEV_OK) return rc;
   } else {
   // Segment k-1 is recomputed (stream rs, record set (k-1)&1) while segment k
   // is reversed (engine stream, record set k&1), when the second set exists.
@@ -3224,17 +3323,26 @@ int lev_adj_backward(LevAdjoint *a, const float *dLdr, const float *dLdtheta,
 }
 
 int lev_adj_grid_info(const LevAdjoint *a, int32_t *eligible, int32_t *enabled,
-                      int32_t *rows_per_cta, int32_t *eligible_rows_mask) {
+                      int32_t *rows_per_cta, int32_t *eligible_rows_mask, int32_t *paired) {
   if (!a) return fail(LEV_ERR_ARG, "null handle");
   if (eligible) *eligible = a->grid_ok ? 1 : 0;
   if (enabled) *enabled = adj_grid_on(a) ? 1 : 0;
   if (rows_per_cta) *rows_per_cta = a->grid_ok ? a->grid_R : 0;
+  if (paired)
+    *paired = (adj_grid_on(a) && a->use_pair && a->ring2 != nullptr &&
+               a->gp_ok[grid_r_index(a->grid_R)]) ? 1 : 0;
   if (eligible_rows_mask) {
     int m = 0;
     for (int i = 0; i < 3; ++i)
       if (a->gR_ok[i]) m |= kGridRs[i];
     *eligible_rows_mask = m;
   }
+  return LEV_OK;
+}
+
+int lev_adj_set_grid_pairing(LevAdjoint *a, int32_t enabled) {
+  if (!a) return fail(LEV_ERR_ARG, "null handle");
+  a->use_pair = enabled != 0;
   return LEV_OK;
 }
 

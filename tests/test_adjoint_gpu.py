@@ -42,12 +42,15 @@ def _params_gpu(net, dev="cuda", K=1.5, nets=1):
     return om, w0, K
 
 
-def _gpu_grads(net, T, math_mode="accurate", segment=50, grid=None):
+def _gpu_grads(net, T, math_mode="accurate", segment=50, grid=None, paired=None):
     eng = LeviathanEngine(*net.engine_args(), math_mode=math_mode)
     adj = Adjoint(eng, segment=segment, max_steps=T)
     if grid is not None:  # False: per-step launches; R: grid-resident, R rows per CTA
         adj.set_grid_mode(bool(grid), int(grid) if grid else 0)
         assert adj.grid_info()["enabled"] == bool(grid)
+    if paired is not None:  # recompute k-1 and reverse k in one launch, or not
+        adj.set_grid_pairing(paired)
+        assert adj.grid_info()["paired"] == paired
     om, w0, K = _params_gpu(net)
     r = simulate(adj, om, w0, K, T, DT)[:, 0]
     tgt = torch.tensor(target_sinusoid(T), dtype=torch.float32, device="cuda")
@@ -122,9 +125,11 @@ def test_segment_length_does_not_change_gradients():
                                              (3000, 32, 64, "accurate")])
 def test_grid_segments_equal_per_step_launches(N, k, md, math_mode):
     """Grid-resident segments (one cooperative launch per checkpoint segment
-    forward and backward) against per-step launches: the forward bitwise, the
-    gradients to summation order (adjoint-ring atomics, row and CTA sums), for
-    every eligible rows-per-CTA choice; a zero-delay network included."""
+    forward and backward, the backward recompute paired with the reverse of
+    the segment after it, or not) against per-step launches: the forward
+    bitwise, the gradients to summation order (adjoint-ring atomics, row and
+    CTA sums), for every eligible rows-per-CTA choice; a zero-delay network
+    included."""
     net = make_network(N, k, 0.1, md, seed=N + k, delay_lo=min(1, md))
     T = 120
     ref = _gpu_grads(net, T, math_mode, segment=50, grid=False)
@@ -133,13 +138,14 @@ def test_grid_segments_equal_per_step_launches(N, k, md, math_mode):
     info = adj.grid_info()
     adj.close()
     eng.close()
-    assert info["eligible"] and info["eligible_rows"], info
-    for R in info["eligible_rows"]:
-        got = _gpu_grads(net, T, math_mode, segment=50, grid=R)
+    assert info["eligible"] and info["eligible_rows"] and info["paired"], info
+    runs = [(R, True) for R in info["eligible_rows"]] + [(info["eligible_rows"][0], False)]
+    for R, paired in runs:
+        got = _gpu_grads(net, T, math_mode, segment=50, grid=R, paired=paired)
         np.testing.assert_array_equal(got[4], ref[4], err_msg=f"R={R}")
         assert got[0] == ref[0]
         for x, y in zip(got[1:4], ref[1:4]):
-            assert _rel(x, y) < 1e-5, (R, _rel(x, y))
+            assert _rel(x, y) < 1e-5, (R, paired, _rel(x, y))
 
 
 def test_drive_and_phase_output_gradients():
