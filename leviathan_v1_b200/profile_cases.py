@@ -2,7 +2,9 @@
 
     python -m leviathan_v1_b200.profile_cases step      [--N 1000000 --k 32 --steps 5]
     python -m leviathan_v1_b200.profile_cases cluster   [--N 1000 --k 20 --steps 200]
+    python -m leviathan_v1_b200.profile_cases grid      [--N 10000 --k 20 --steps 200]
     python -m leviathan_v1_b200.profile_cases adjoint   [--N 200000 --k 32 --T 100]
+    python -m leviathan_v1_b200.profile_cases adjgrid   [--N 10000 --k 20 --T 200]
     python -m leviathan_v1_b200.profile_cases reservoir [--N 20000 --batch 8 --T 60]
     python -m leviathan_v1_b200.profile_cases e2e       [--N 1000000 --k 32 --steps 500]
 
@@ -59,6 +61,24 @@ def case_cluster(a):
     return dict(case="cluster", N=a.N, E=net.E, steps=a.steps, s=dt, cluster=info)
 
 
+def case_grid(a):
+    from .engine import LeviathanEngine
+    from .graphs import make_network_gpu
+
+    net = make_network_gpu(a.N, a.k, 0.1, a.max_delay, a.seed)
+    e = LeviathanEngine(*net.engine_args())
+    e.set_cluster_mode(False)
+    e.set_grid_mode(True, 64)
+    info = e.grid_info()
+    e.step_n(0.05, 3)
+    _sync()
+    t = time.perf_counter()
+    e.step_n(0.05, a.steps)
+    dt = time.perf_counter() - t
+    e.close()
+    return dict(case="grid", N=a.N, E=net.E, steps=a.steps, s=dt, grid=info)
+
+
 def case_adjoint(a):
     import torch
 
@@ -78,8 +98,8 @@ def case_adjoint(a):
     (r ** 2).mean().backward()
     _sync()
     dt = time.perf_counter() - t
-    out = dict(case="adjoint", N=a.N, E=net.E, T=a.T, segment=a.segment, s=dt,
-               device_bytes=adj.device_bytes)
+    out = dict(case=a.case, N=a.N, E=net.E, T=a.T, segment=a.segment, s=dt,
+               device_bytes=adj.device_bytes, grid=adj.grid_info())
     adj.close()
     eng.close()
     return out
@@ -134,10 +154,13 @@ def case_e2e(a):
                 snapshot_s=t3 - t2, step_n_per_step_us=(t4 - t3) / a.steps * 1e6)
 
 
-CASES = dict(step=case_step, cluster=case_cluster, adjoint=case_adjoint,
+CASES = dict(step=case_step, cluster=case_cluster, grid=case_grid, adjoint=case_adjoint,
+             adjgrid=case_adjoint,
              reservoir=case_reservoir, e2e=case_e2e)
 DEFAULTS = dict(step=dict(N=1_000_000, k=32, max_delay=64, steps=5),
                 cluster=dict(N=1000, k=20, max_delay=50, steps=200),
+                grid=dict(N=10_000, k=20, max_delay=50, steps=200),
+                adjgrid=dict(N=10_000, k=20, max_delay=50, T=200),
                 adjoint=dict(N=200_000, k=32, max_delay=50, T=100),
                 reservoir=dict(N=20_000, k=20, max_delay=50, T=60, batch=8),
                 e2e=dict(N=1_000_000, k=32, max_delay=64, steps=500))
@@ -150,9 +173,9 @@ def main(argv=None):
                       ("T", int), ("batch", int), ("segment", int), ("seed", int)):
         ap.add_argument(f"--{name}", type=typ, default=None)
     a = ap.parse_args(argv)
-    d = dict(DEFAULTS[a.case], segment=50, seed=0)
+    d = dict(DEFAULTS[a.case], segment=50, seed=0, case=a.case)
     for k_, v in vars(a).items():
-        if v is not None and k_ != "case":
+        if v is not None:
             d[k_] = v
     for k_, v in d.items():
         setattr(a, k_, v)
