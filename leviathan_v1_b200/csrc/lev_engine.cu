@@ -8,6 +8,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <atomic>
 #include <cmath>
 #include <cstdio>
 #include <cstring>
@@ -15,6 +16,7 @@
 #include <map>
 #include <mutex>
 #include <string>
+#include <thread>
 #include <tuple>
 #include <vector>
 
@@ -852,6 +854,94 @@ int write_state(LevEngine *h, int n, const NetState &s) {
   return LEV_OK;
 }
 
+// Host-to-device upload of a caller's (usually pageable) array.  The driver
+// copies pageable memory through its own staging at one host thread's memcpy
+// speed; here the host side is split over several threads, each filling a
+// pinned staging buffer of its own and issuing the DMA of that chunk on the
+// engine's stream while it fills the next.  The staging buffers (kStageBufs x
+// kStageBytes of pinned memory) are allocated on the first large upload of
+// the process and kept for later ones.  Small or already pinned sources take
+// one cudaMemcpyAsync.  The source is fully read when this returns.
+constexpr size_t kStageBytes = 4u << 20;
+constexpr int kStageBufs = 8;
+struct StagePool {
+  std::mutex mu;
+  int device = -1;  // device of the events
+  int nbuf = 0;
+  void *buf[kStageBufs] = {};
+  cudaEvent_t ev[kStageBufs] = {};
+};
+static StagePool g_stage;
+
+cudaError_t upload(void *dst, const void *src, size_t bytes, cudaStream_t s) {
+  if (bytes < 2 * kStageBytes)
+    return cudaMemcpyAsync(dst, src, bytes, cudaMemcpyHostToDevice, s);
+  cudaPointerAttributes at;
+  if (cudaPointerGetAttributes(&at, src) != cudaSuccess) {
+    cudaGetLastError();
+    at.type = cudaMemoryTypeUnregistered;
+  }
+  if (at.type != cudaMemoryTypeUnregistered)
+    return cudaMemcpyAsync(dst, src, bytes, cudaMemcpyHostToDevice, s);
+  int dev = 0;
+  cudaError_t ce = cudaGetDevice(&dev);
+  if (ce != cudaSuccess) return ce;
+  std::lock_guard<std::mutex> lk(g_stage.mu);
+  if (g_stage.nbuf > 0 && g_stage.device != dev)  // the events belong to another device
+    return cudaMemcpyAsync(dst, src, bytes, cudaMemcpyHostToDevice, s);
+  if (g_stage.nbuf == 0) {
+    g_stage.device = dev;
+    const unsigned hw = std::thread::hardware_concurrency();
+    const int want = (int)std::max(2u, std::min<unsigned>(kStageBufs, hw / 2));
+    for (int b = 0; b < want; ++b) {
+      if (cudaHostAlloc(&g_stage.buf[b], kStageBytes,
+                        cudaHostAllocPortable) != cudaSuccess ||
+          cudaEventCreateWithFlags(&g_stage.ev[b], cudaEventDisableTiming) != cudaSuccess) {
+        cudaGetLastError();
+        if (g_stage.buf[b]) cudaFreeHost(g_stage.buf[b]);
+        g_stage.buf[b] = nullptr;
+        break;
+      }
+      // a first wait on the event returns at once
+      cudaEventRecord(g_stage.ev[b], s);
+      g_stage.nbuf = b + 1;
+    }
+    if (g_stage.nbuf < 2) return cudaMemcpyAsync(dst, src, bytes, cudaMemcpyHostToDevice, s);
+  }
+  const long long nchunks = (long long)((bytes + kStageBytes - 1) / kStageBytes);
+  std::atomic<long long> next{0};
+  std::atomic<int> failed{(int)cudaSuccess};
+  auto worker = [&](int b) {
+    if (cudaSetDevice(dev) != cudaSuccess) {
+      failed = (int)cudaErrorInvalidDevice;
+      return;
+    }
+    for (;;) {
+      const long long c = next++;
+      if (c >= nchunks || failed != (int)cudaSuccess) break;
+      const size_t off = (size_t)c * kStageBytes;
+      const size_t n = std::min(kStageBytes, bytes - off);
+      cudaError_t e = cudaEventSynchronize(g_stage.ev[b]);  // its last DMA is done
+      if (e == cudaSuccess) {
+        std::memcpy(g_stage.buf[b], static_cast<const char *>(src) + off, n);
+        e = cudaMemcpyAsync(static_cast<char *>(dst) + off, g_stage.buf[b], n,
+                            cudaMemcpyHostToDevice, s);
+      }
+      if (e == cudaSuccess) e = cudaEventRecord(g_stage.ev[b], s);
+      if (e != cudaSuccess) {
+        failed = (int)e;
+        break;
+      }
+    }
+  };
+  const int nth = (int)std::min<long long>(g_stage.nbuf, nchunks);
+  std::vector<std::thread> th;
+  for (int b = 1; b < nth; ++b) th.emplace_back(worker, b);
+  worker(0);
+  for (auto &t : th) t.join();
+  return (cudaError_t)failed.load();
+}
+
 int create_impl(LevEngine **out, int num_nets, const int32_t *Ns,
                 const int32_t *mds, const int32_t *rp_cat,
                 const int32_t *col_cat, const uint8_t *d_cat,
@@ -1088,8 +1178,7 @@ int create_impl(LevEngine **out, int num_nets, const int32_t *Ns,
   };
 #define LEV_UP(dst, src, bytes)                                            \
   do {                                                                     \
-    cudaError_t _e = cudaMemcpyAsync((dst), (src), (bytes),                \
-                                     cudaMemcpyHostToDevice, h->stream);   \
+    cudaError_t _e = upload((dst), (src), (bytes), h->stream);             \
     if (_e != cudaSuccess)                                                 \
       return cleanup_fail(LEV_ERR_CUDA, std::string("upload failed: ") +   \
                                             cudaGetErrorString(_e));       \
