@@ -9,9 +9,14 @@
 //     and its rows of every ring slot live in its shared memory;
 //   * a delayed phase of a node owned by another CTA is read from that CTA's
 //     shared memory (distributed shared memory, cluster.map_shared_rank);
-//   * one cluster barrier per step orders every ring write before the next
-//     step's reads (with max_delay+2 ring slots, reads and the write of one
-//     step never touch the same slot);
+//   * one cluster barrier per step, split into an arrival after step t's
+//     ring write and warp sums and a wait before step t+1's integrate (which
+//     needs g(t+1) and overwrites ring slot t+2 = t-max_delay, read by step
+//     t).  Without zero delays step t+1's gathers read slots <= t, ordered by
+//     the barrier of step t-1, so the predictor and the edge work of step t+1
+//     run while the barrier of step t completes; with zero delays the wait
+//     comes before the gathers (with max_delay+2 ring slots, reads and the
+//     write of one step never touch the same slot);
 //   * each warp's shuffle-tree (sum cos, sum sin) of its 32 rows goes to a
 //     double-buffered array in CTA 0; after the barrier every CTA forms the
 //     256-node block sums from eight warp sums with the arithmetic of the
@@ -88,8 +93,18 @@ struct ClusterArgs {
   int R;          // rows per CTA (a power of two, 32 .. 1024)
   int lgR;        // log2(R)
   int edge_cap;   // SELL entries per CTA the shared memory was sized for
+  int early;      // no delay is 0: wait for step t's barrier after step t+1's edges
   float dt;
 };
+
+// Split cluster barrier (every thread of every CTA of the cluster): arrival
+// with release semantics, wait with acquire semantics.
+__device__ __forceinline__ void cluster_arrive() {
+  asm volatile("barrier.cluster.arrive.release.aligned;" ::: "memory");
+}
+__device__ __forceinline__ void cluster_wait() {
+  asm volatile("barrier.cluster.wait.acquire.aligned;" ::: "memory");
+}
 
 // shared memory layout (bytes, from the dynamic base):
 //   wsum   float2 [2][kClusterWarpsMax]        warp sums (used in CTA 0)
@@ -176,27 +191,8 @@ __global__ void __launch_bounds__(MAXR, 1) cluster_kernel(const ClusterArgs a) {
   float2 *wsum0 = cluster.map_shared_rank(wsum, 0);
   __shared__ float s_g;
   for (int step = 0; step < a.n_steps; ++step) {
-    // ---- r and gain of the previous step: warp 0 of every CTA reduces the
-    // block partials (same order everywhere) and shares g with its CTA ----
-    if (step > 0) {
-      if (warp == 0) {
-        const float2 sums =
-            cluster_sums(wsum0 + ((step - 1) & 1) * kClusterWarpsMax, nblocks, lane);
-        const float sum_cos = sums.x, sum_sin = sums.y;
-        if (lane == 0) {
-          float inv_N = 1.0f / (float)N;
-          r = sqrtf(sum_cos * sum_cos + sum_sin * sum_sin) * inv_N;
-          if (nd.ctrl) g = gain_controller(g, r, dt, nd);
-          s_g = g;
-          if (rank == 0 && a.r_hist) {
-            const int k = ns.rpos + step - 1;
-            if (k < a.r_cap) a.r_hist[k] = r;
-          }
-        }
-      }
-      __syncthreads();
-      g = s_g;
-    }
+    // with zero delays: step-1's barrier before the gathers
+    if (step > 0 && !a.early) cluster_wait();
     // ---- predictor --------------------------------------------------------
     float th = 0.0f, eps = 0.0f;
     if (live) {
@@ -253,6 +249,28 @@ __global__ void __launch_bounds__(MAXR, 1) cluster_kernel(const ClusterArgs a) {
         }
       }
     }
+    // ---- r and gain of the previous step: warp 0 of every CTA reduces the
+    // block partials (same order everywhere) and shares g with its CTA ----
+    if (step > 0) {
+      if (a.early) cluster_wait();
+      if (warp == 0) {
+        const float2 sums =
+            cluster_sums(wsum0 + ((step - 1) & 1) * kClusterWarpsMax, nblocks, lane);
+        const float sum_cos = sums.x, sum_sin = sums.y;
+        if (lane == 0) {
+          float inv_N = 1.0f / (float)N;
+          r = sqrtf(sum_cos * sum_cos + sum_sin * sum_sin) * inv_N;
+          if (nd.ctrl) g = gain_controller(g, r, dt, nd);
+          s_g = g;
+          if (rank == 0 && a.r_hist) {
+            const int k = ns.rpos + step - 1;
+            if (k < a.r_cap) a.r_hist[k] = r;
+          }
+        }
+      }
+      __syncthreads();
+      g = s_g;
+    }
     // ---- integrate ----------------------------------------------------------
     int nxt = cur + 1;
     if (nxt == bsi) nxt = 0;
@@ -277,8 +295,9 @@ __global__ void __launch_bounds__(MAXR, 1) cluster_kernel(const ClusterArgs a) {
       wsum0[(step & 1) * kClusterWarpsMax + row0 / 32 + warp] = make_float2(my_cos, my_sin);
     cur = nxt;
     rbuf = (rbuf + 1 == nd.max_delay + 1) ? 0 : rbuf + 1;
-    cluster.sync();
+    cluster_arrive();
   }
+  if (a.n_steps > 0) cluster_wait();
   // ---- r of the last step, then write the state back ------------------------
   if (a.n_steps > 0) {
     const float2 sums =
@@ -408,24 +427,8 @@ __global__ void __launch_bounds__(4 * 128, 1) cluster_split_kernel(const Cluster
   float2 *wsum0 = cluster.map_shared_rank(wsum, 0);
   __shared__ float s_g;
   for (int step = 0; step < a.n_steps; ++step) {
-    if (step > 0) {
-      if (warp == 0) {
-        const float2 sums =
-            cluster_sums(wsum0 + ((step - 1) & 1) * kClusterWarpsMax, nblocks, lane);
-        if (lane == 0) {
-          float inv_N = 1.0f / (float)N;
-          r = sqrtf(sums.x * sums.x + sums.y * sums.y) * inv_N;
-          if (nd.ctrl) g = gain_controller(g, r, dt, nd);
-          s_g = g;
-          if (rank == 0 && a.r_hist) {
-            const int k = ns.rpos + step - 1;
-            if (k < a.r_cap) a.r_hist[k] = r;
-          }
-        }
-      }
-      __syncthreads();
-      g = s_g;
-    }
+    // with zero delays: step-1's barrier before the gathers
+    if (step > 0 && !a.early) cluster_wait();
     // ---- predictor (row's first lane) --------------------------------------
     float th = 0.0f, eps = 0.0f;
     if (live && q == 0) {
@@ -494,6 +497,26 @@ __global__ void __launch_bounds__(4 * 128, 1) cluster_split_kernel(const Cluster
         }
       }
     }
+    // ---- r and gain of the previous step (warp 0 of every CTA) -------------
+    if (step > 0) {
+      if (a.early) cluster_wait();
+      if (warp == 0) {
+        const float2 sums =
+            cluster_sums(wsum0 + ((step - 1) & 1) * kClusterWarpsMax, nblocks, lane);
+        if (lane == 0) {
+          float inv_N = 1.0f / (float)N;
+          r = sqrtf(sums.x * sums.x + sums.y * sums.y) * inv_N;
+          if (nd.ctrl) g = gain_controller(g, r, dt, nd);
+          s_g = g;
+          if (rank == 0 && a.r_hist) {
+            const int k = ns.rpos + step - 1;
+            if (k < a.r_cap) a.r_hist[k] = r;
+          }
+        }
+      }
+      __syncthreads();
+      g = s_g;
+    }
     // ---- integrate (row's first lane) --------------------------------------
     int nxt = cur + 1;
     if (nxt == bsi) nxt = 0;
@@ -525,8 +548,9 @@ __global__ void __launch_bounds__(4 * 128, 1) cluster_split_kernel(const Cluster
     }
     cur = nxt;
     rbuf = (rbuf + 1 == nd.max_delay + 1) ? 0 : rbuf + 1;
-    cluster.sync();
+    cluster_arrive();
   }
+  if (a.n_steps > 0) cluster_wait();
   // ---- r of the last step, then write the state back ------------------------
   if (a.n_steps > 0) {
     const float2 sums =

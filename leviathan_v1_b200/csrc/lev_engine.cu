@@ -592,6 +592,7 @@ int launch_cluster(LevEngine *h, float dt, int len) {
   ca.lgR = 0;
   while ((1 << ca.lgR) < h->cluster_R) ++ca.lgR;
   ca.edge_cap = h->cluster_edge_cap;
+  ca.early = h->pair_ok ? 1 : 0;  // no delay is 0
   ca.dt = dt;
   cudaLaunchConfig_t cfg = {};
   cfg.gridDim = dim3(h->cluster_C);
