@@ -56,6 +56,14 @@ struct AdjGridFwdArgs {
   float2 *wsum;        // [2][nwarps]
   unsigned *bar;
   int *err;
+  // the segment's checkpoint (theta, theta_hat, omega_hat, SELL weights, the
+  // last max_delay+1 ring slots as [m][N], g): ck_mode 1 writes it from the
+  // initial state (forward pass); 2 takes the initial state from it and
+  // refills ring slots 0..max_delay, the unwrapped segment ring (backward
+  // recompute), then w0_out (if not null) receives the initial weights
+  int ck_mode;
+  float *ck_theta, *ck_thh, *ck_omh, *ck_w, *ck_ring, *ck_g;
+  float *w0_out;
   long long SL;
   int early;           // no delay is 0
   int nwarps;
@@ -115,23 +123,58 @@ __device__ __forceinline__ void adj_grid_fwd_body(const AdjGridFwdArgs &a, const
   }
   if (my_slices) eend = a.sl_off[sl0 + my_slices - 1] + 32LL * a.sl_len[sl0 + my_slices - 1];
   const int nent = (int)(eend - ebase);
+  const bool restore = a.ck_mode == 2;
+  const float *w_src = restore ? a.ck_w : a.w_in;
   for (int k = tid; k < nent; k += blockDim.x) {
     s_cd[k] = a.sl_cd[ebase + k];
-    s_w[k] = a.w_in[ebase + k];
+    const float w = w_src[ebase + k];
+    s_w[k] = w;
+    if (a.ck_mode == 1) a.ck_w[ebase + k] = w;
+    if (restore && a.w0_out) a.w0_out[ebase + k] = w;
   }
   const long long gi = nd.node_off + row;
   int deg = 0;
   if (live) {
     if (q == 0) {
-      s_th[rloc] = a.theta[gi];
-      s_thh[rloc] = a.theta_hat[gi];
+      const float th0 = restore ? a.ck_theta[gi] : a.theta[gi];
+      const float thh0 = restore ? a.ck_thh[gi] : a.theta_hat[gi];
+      const float omh0 = restore ? a.ck_omh[gi] : a.omega_hat[gi];
+      s_th[rloc] = th0;
+      s_thh[rloc] = thh0;
       s_om[rloc] = a.omega[gi];
-      s_omh[rloc] = a.omega_hat[gi];
+      s_omh[rloc] = omh0;
+      if (a.ck_mode == 1) {
+        a.ck_theta[gi] = th0;
+        a.ck_thh[gi] = thh0;
+        a.ck_omh[gi] = omh0;
+      }
     }
     const int *rp = a.row_ptr + nd.rp_off + row;
     deg = rp[1] - rp[0];
   }
-  const NetState ns = *a.st;
+  NetState ns;
+  if (restore) {
+    // the state of a restored segment (adj_state_kernel mode 2)
+    ns.g = a.ck_g[0];
+    ns.r = 0.0f;
+    ns.cur = nd.max_delay;
+    ns.ticket = 0u;
+    ns.t = 0;
+    ns.rbuf = 0;
+    ns.rpos = 0;
+  } else {
+    ns = *a.st;
+  }
+  if (a.ck_mode == 1) {
+    // ring window: theta(t - m) -> ck_ring[m][N], m = 0..max_delay
+    if (live)
+      for (int m = q; m <= nd.max_delay; m += LPR) {
+        int slot = ns.cur - m;
+        slot += (slot < 0) ? nd.bsi : 0;
+        a.ck_ring[(long long)m * N + row] = a.ring[nd.ring_off + (long long)slot * nd.Np + row];
+      }
+    if (cta == 0 && tid == 0) a.ck_g[0] = ns.g;
+  }
   int cur = ns.cur;
   float g = ns.g, r = ns.r;
   const int nblocks = (N + kTile - 1) / kTile;
@@ -144,6 +187,17 @@ __device__ __forceinline__ void adj_grid_fwd_body(const AdjGridFwdArgs &a, const
   const bool slice_live = row0 + wslice * 32 < N;
   if (tid == 0) s_ok = 1;
   __syncthreads();
+  // restored segment: theta(s0 - m) -> ring slot max_delay - m of every row,
+  // read by every CTA's first gathers: one grid barrier before step 0
+  unsigned base = 0;
+  if (restore) {
+    if (live)
+      for (int m = q; m <= nd.max_delay; m += LPR)
+        __stcg(ring_w + (long long)(nd.max_delay - m) * Np + row, a.ck_ring[(long long)m * N + row]);
+    grid_arrive(a.bar);
+    if (!grid_wait(a.bar, G, a.err, &s_ok)) return;
+    base = G;
+  }
 
   auto stage_sums = [&](int s) {
     if (warp == 0) {
@@ -177,7 +231,7 @@ __device__ __forceinline__ void adj_grid_fwd_body(const AdjGridFwdArgs &a, const
   bool ok = true;
   for (; step < a.n_steps; ++step) {
     if (step > 0 && !a.early) {
-      if (!(ok = grid_wait(a.bar, (unsigned)step * G, a.err, &s_ok))) break;
+      if (!(ok = grid_wait(a.bar, base + (unsigned)step * G, a.err, &s_ok))) break;
       stage_sums(step - 1);
     }
     // ---- predictor (row's first lane) --------------------------------------
@@ -247,7 +301,7 @@ __device__ __forceinline__ void adj_grid_fwd_body(const AdjGridFwdArgs &a, const
     }
     if (step > 0) {
       if (a.early) {
-        if (!(ok = grid_wait(a.bar, (unsigned)step * G, a.err, &s_ok))) break;
+        if (!(ok = grid_wait(a.bar, base + (unsigned)step * G, a.err, &s_ok))) break;
         stage_sums(step - 1);
       }
       reduce_prev(step);
@@ -298,7 +352,8 @@ __device__ __forceinline__ void adj_grid_fwd_body(const AdjGridFwdArgs &a, const
     cur = nxt;
     grid_arrive(a.bar);
   }
-  if (ok && a.n_steps > 0 && cta == 0) ok = grid_wait(a.bar, (unsigned)a.n_steps * G, a.err, &s_ok);
+  if (ok && a.n_steps > 0 && cta == 0)
+    ok = grid_wait(a.bar, base + (unsigned)a.n_steps * G, a.err, &s_ok);
   if (!ok) return;
   if (a.n_steps > 0 && cta == 0 && warp == 0) {
     const float2 *src = a.wsum + ((a.n_steps - 1) & 1) * nwarps;

@@ -2801,6 +2801,18 @@ int adj_setup_grid(LevAdjoint *a, const std::vector<long long> &sl_off,
   return LEV_OK;
 }
 
+// The checkpoint slots of segment `seg` for a grid-resident forward launch
+// (mode 1: written from the initial state; 2: the initial state).
+void adj_grid_ckpt_args(LevAdjoint *a, int seg, int mode, AdjGridFwdArgs &g) {
+  g.ck_mode = mode;
+  g.ck_theta = a->ck_theta + (size_t)seg * a->TN;
+  g.ck_thh = a->ck_thh + (size_t)seg * a->TN;
+  g.ck_omh = a->ck_omh + (size_t)seg * a->TN;
+  g.ck_w = a->ck_w + (size_t)seg * a->SL;
+  g.ck_ring = a->ck_ring + (size_t)seg * a->ckr_floats;  // one network: offset 0
+  g.ck_g = a->ck_g + (size_t)seg * a->NN;
+}
+
 inline bool adj_grid_on(const LevAdjoint *a) {
   return a->grid_ok && a->use_grid && a->res_ra == nullptr;
 }
@@ -3105,13 +3117,13 @@ int lev_adj_forward(LevAdjoint *a, float dt, int32_t T, const float *omega,
   adj_state_kernel<<<1, 128, 0, s>>>(0, a->d_nets, a->d_st, nullptr, K, a->NN);
   LEV_TRY_CUDA(cudaGetLastError());
   if (adj_grid_on(a)) {
-    // one cooperative launch per checkpoint segment
+    // one cooperative launch per checkpoint segment, which also writes the
+    // segment's checkpoint
     for (int t0 = 0; t0 < T; t0 += a->C) {
       const int n = std::min(a->C, T - t0);
-      int rc = adj_ckpt(a, t0 / a->C, true);
-      if (rc != LEV_OK) return rc;
       AdjGridFwdArgs g;
       std::memset(&g, 0, sizeof(g));
+      adj_grid_ckpt_args(a, t0 / a->C, 1, g);
       g.w_in = a->w;
       g.w_out = a->w;
       g.ring = a->ring;
@@ -3123,7 +3135,7 @@ int lev_adj_forward(LevAdjoint *a, float dt, int32_t T, const float *omega,
       g.r_out = r_out + (size_t)t0 * a->NN;
       g.theta_out = theta_out ? theta_out + (size_t)t0 * a->TN : nullptr;
       g.dt = dt;
-      rc = adj_grid_launch_fwd(a, g, n, s);
+      int rc = adj_grid_launch_fwd(a, g, n, s);
       if (rc != LEV_OK) return rc;
     }
     LEV_TRY_CUDA(cudaStreamSynchronize(s));
@@ -3201,13 +3213,13 @@ int lev_adj_backward(LevAdjoint *a, const float *dLdr, const float *dLdtheta,
     float *ths[2] = {a->thh_hist, two ? a->thh_hist2 : a->thh_hist};
     float4 *trs[2] = {a->trace, two ? a->trace2 : a->trace};
     auto seg_len = [&](int seg) { return std::min(T, seg * a->C + a->C) - seg * a->C; };
-    // restore segment `seg` and describe its recompute into its record set
+    // the recompute of segment `seg` (restored from its checkpoint by the
+    // launch itself) into its record set
     auto prep_fwd = [&](int seg, AdjGridFwdArgs &g) -> int {
       const int s0 = seg * a->C, n = seg_len(seg), k = paired ? (seg & 1) : 0;
-      int rc = adj_ckpt(a, seg, false, s, rings[k]);
-      if (rc != LEV_OK) return rc;
-      LEV_TRY_CUDA(cudaMemcpyAsync(whs[k], a->w, wb, cudaMemcpyDeviceToDevice, s));
       std::memset(&g, 0, sizeof(g));
+      adj_grid_ckpt_args(a, seg, 2, g);
+      g.w0_out = whs[k];
       g.w_in = whs[k];
       g.w_rec = whs[k] + a->SL;
       g.w_out = whs[k] + (size_t)n * a->SL;
