@@ -173,6 +173,15 @@ struct LevEngine {
   bool pair_ok = false;
   bool use_pairs = true;
   float2 *d_pend = nullptr;  // [total_nodes] parked (coupling sum, eps)
+  // speculative pairs of single steps (lev_step): the first call runs the
+  // pair kernel with step t+1's weights and predictor going to the spec
+  // buffers and returns r(t+1); the next call, if nothing wrote the engine
+  // state in between and dt is the same, only finishes step t+1 and swaps the
+  // weight buffers (w_flip tells which one is current, for the graph cache)
+  bool spec = false;
+  uint32_t spec_dt = 0;  // bits of the dt of the pending step
+  float *d_w_spec = nullptr, *d_thh_spec = nullptr, *d_omh_spec = nullptr;
+  int w_flip = 0;
   int *d_class_nets = nullptr;  // networks of each class, class by class
   LevHubs *hubs = nullptr;      // attached hub monitor (lev_attach_hubs)
   // step blocks of engines with several degree classes: one chain of
@@ -270,6 +279,9 @@ void free_engine(LevEngine *h) {
   cudaFree(h->d_ring);
   cudaFree(h->d_part);
   cudaFree(h->d_pend);
+  cudaFree(h->d_w_spec);
+  cudaFree(h->d_thh_spec);
+  cudaFree(h->d_omh_spec);
   cudaFree(h->d_class_nets);
   cudaFree(h->d_rhist);
   cudaFree(h->d_gwsum);
@@ -368,6 +380,9 @@ StepArgs make_args(LevEngine *h, float dt, float *r_hist, int r_cap,
   a.reverse = 0;
   a.pend = h->d_pend;
   a.hubs = h->hubs ? h->hubs->d_mon : nullptr;
+  a.w2 = nullptr;
+  a.thh2 = nullptr;
+  a.omh2 = nullptr;
   return a;
 }
 
@@ -471,6 +486,20 @@ int launch_two_steps(LevEngine *h, StepArgs a) {
   return LEV_OK;
 }
 
+// Every class of the engine takes two steps per launch (speculative pairs
+// need it: a class stepped by step_kernel updates the weights in place).
+bool pairs_all(const LevEngine *h) {
+  if (!h->pair_ok || !h->use_pairs) return false;
+  for (int c = 0; c < kNumClasses; ++c)
+    if (h->classes[c].ntiles > 0 && h->classes[c].pair_variant < 0) return false;
+  return true;
+}
+
+// Anything that writes the engine state (or the kernels' configuration)
+// drops a pending speculative step; the state itself is that after the last
+// completed step.
+inline void spec_drop(LevEngine *h) { h->spec = false; }
+
 void clear_graphs(LevEngine *h) {
   for (auto &kv : h->graphs) {
     if (kv.second.exec) cudaGraphExecDestroy(kv.second.exec);
@@ -483,7 +512,7 @@ void clear_graphs(LevEngine *h) {
 int get_graph(LevEngine *h, int len, float dt, cudaGraphExec_t *out) {
   uint32_t dbits;
   std::memcpy(&dbits, &dt, 4);
-  auto key = std::make_tuple(len, dbits, h->math_mode);
+  auto key = std::make_tuple(len, dbits, h->math_mode + 2 * h->w_flip);
   auto it = h->graphs.find(key);
   if (it != h->graphs.end()) {
     *out = it->second.exec;
@@ -813,6 +842,7 @@ int check_grid_error(LevEngine *h) {
 // networks); if stage != null, the r history of every block is copied into
 // stage[n][num_nets] (pinned host memory).
 int enqueue_steps(LevEngine *h, float dt, int n, float *stage) {
+  spec_drop(h);
   int done = 0;
   while (done < n) {
     const int len = std::min(h->block_len, n - done);
@@ -1380,8 +1410,48 @@ int lev_step(LevEngine *h, float dt, float *r_out) {
   if (!std::isfinite(dt)) return fail(LEV_ERR_ARG, "dt is not finite");
   DeviceScope ds(h->device);
   StepArgs a = make_args(h, dt, nullptr, 0, h->d_rmap);
-  int rc = launch_step(h, a);
-  if (rc != LEV_OK) return rc;
+  int rc = LEV_OK;
+  uint32_t dbits;
+  std::memcpy(&dbits, &dt, 4);
+  if (pairs_all(h)) {
+    if (h->spec && h->spec_dt == dbits) {
+      // the speculative step t+1: its integrate, then the weights it wrote
+      a.thh2 = h->d_thh_spec;
+      a.omh2 = h->d_omh_spec;
+      a.reverse = h->sweep;
+      h->sweep ^= 1;
+      for (int c = 0; c < kNumClasses && rc == LEV_OK; ++c) rc = launch_pair_class(h, c, a, 1);
+      h->spec = false;
+      if (rc != LEV_OK) return rc;
+      std::swap(h->d_sl_w, h->d_w_spec);
+      h->w_flip ^= 1;
+    } else {
+      h->spec = false;
+      if (!h->d_w_spec) {
+        rc = dev_alloc(h, &h->d_w_spec, (size_t)std::max<long long>(h->sl_total, 1));
+        if (rc == LEV_OK) rc = dev_alloc(h, &h->d_thh_spec, (size_t)h->total_nodes);
+        if (rc == LEV_OK) rc = dev_alloc(h, &h->d_omh_spec, (size_t)h->total_nodes);
+        if (rc != LEV_OK) return rc;
+        // padding entries (never written by a walk) as in the live buffer
+        LEV_TRY_CUDA(cudaMemcpyAsync(h->d_w_spec, h->d_sl_w,
+                                     sizeof(float) * std::max<long long>(h->sl_total, 1),
+                                     cudaMemcpyDeviceToDevice, h->stream));
+      }
+      // step t in full and step t+1 up to its integrate, into the spec buffers
+      a.w2 = h->d_w_spec;
+      a.thh2 = h->d_thh_spec;
+      a.omh2 = h->d_omh_spec;
+      a.reverse = h->sweep;
+      h->sweep ^= 1;
+      for (int c = 0; c < kNumClasses && rc == LEV_OK; ++c) rc = launch_pair_class(h, c, a, 0);
+      if (rc != LEV_OK) return rc;
+      h->spec = true;
+      h->spec_dt = dbits;
+    }
+  } else {
+    rc = launch_step(h, a);
+    if (rc != LEV_OK) return rc;
+  }
   LEV_TRY_CUDA(cudaStreamSynchronize(h->stream));
   if (r_out) {
     const volatile float *src = h->h_rmap;
@@ -1471,6 +1541,7 @@ int lev_get_theta_net(LevEngine *h, int32_t net, float *theta_out) {
 }
 
 int lev_set_theta(LevEngine *h, const float *theta_in) {
+  if (h) spec_drop(h);
   if (!h || !theta_in) return fail(LEV_ERR_ARG, "null argument");
   DeviceScope ds(h->device);
   int rc = upload_nodes(h, h->d_theta, theta_in, 0, h->total_nodes);
@@ -1481,6 +1552,7 @@ int lev_set_theta(LevEngine *h, const float *theta_in) {
 }
 
 int lev_set_theta_net(LevEngine *h, int32_t net, const float *theta_in) {
+  if (h) spec_drop(h);
   if (!h || !theta_in) return fail(LEV_ERR_ARG, "null argument");
   if (net < 0 || net >= h->num_nets)
     return fail(LEV_ERR_ARG, "network index out of range");
@@ -1524,6 +1596,7 @@ int lev_get_weights(LevEngine *h, float *w_out) {
 }
 
 int lev_reset_weights(LevEngine *h, const float *w_in) {
+  if (h) spec_drop(h);
   if (!h || (!w_in && h->total_edges > 0))
     return fail(LEV_ERR_ARG, "null argument");
   DeviceScope ds(h->device);
@@ -1573,6 +1646,7 @@ int lev_get_predictor(LevEngine *h, float *theta_hat_out,
 int lev_set_predictor(LevEngine *h, const float *theta_hat_in,
                       const float *omega_hat_in) {
   if (!h) return fail(LEV_ERR_ARG, "null handle");
+  spec_drop(h);
   DeviceScope ds(h->device);
   int rc = LEV_OK;
   if (theta_hat_in)
@@ -1591,6 +1665,7 @@ int lev_get_omega(LevEngine *h, float *omega_out) {
 }
 
 int lev_set_omega(LevEngine *h, const float *omega_in) {
+  if (h) spec_drop(h);
   if (!h || !omega_in) return fail(LEV_ERR_ARG, "null argument");
   DeviceScope ds(h->device);
   int rc = upload_nodes(h, h->d_omega, omega_in, 0, h->total_nodes);
@@ -1628,6 +1703,7 @@ int lev_get_ring(LevEngine *h, int32_t net, float *ring_out,
 
 int lev_set_ring(LevEngine *h, int32_t net, const float *ring_in,
                  int32_t buf_idx) {
+  if (h) spec_drop(h);
   if (!h || !ring_in) return fail(LEV_ERR_ARG, "null argument");
   if (net < 0 || net >= h->num_nets)
     return fail(LEV_ERR_ARG, "network index out of range");
@@ -1727,6 +1803,7 @@ int lev_set_gain_controller(LevEngine *h, int32_t net, int32_t enabled) {
 }
 
 int lev_set_params(LevEngine *h, int32_t net, const LevParams *p) {
+  if (h) spec_drop(h);
   if (!h || !p) return fail(LEV_ERR_ARG, "null argument");
   if (net < -1 || net >= h->num_nets)
     return fail(LEV_ERR_ARG, "network index out of range");
@@ -1764,6 +1841,7 @@ int lev_get_params(LevEngine *h, int32_t net, LevParams *p) {
 
 int lev_set_math_mode(LevEngine *h, int32_t math_mode) {
   if (!h) return fail(LEV_ERR_ARG, "null handle");
+  spec_drop(h);
   if (math_mode != LEV_MATH_REFERENCE && math_mode != LEV_MATH_ACCURATE)
     return fail(LEV_ERR_ARG, "math_mode must be 0 (reference) or 1");
   h->math_mode = math_mode;
@@ -1847,6 +1925,7 @@ int lev_pair_info(const LevEngine *h, int32_t c, int32_t *eligible, int32_t *ena
 
 int lev_set_pair_mode(LevEngine *h, int32_t enabled) {
   if (!h) return fail(LEV_ERR_ARG, "null handle");
+  spec_drop(h);
   if ((enabled != 0) != h->use_pairs) {
     DeviceScope ds(h->device);
     cudaStreamSynchronize(h->stream);
@@ -1858,6 +1937,7 @@ int lev_set_pair_mode(LevEngine *h, int32_t enabled) {
 
 int lev_set_pair_variant(LevEngine *h, int32_t c, int32_t v) {
   if (!h) return fail(LEV_ERR_ARG, "null handle");
+  spec_drop(h);
   if (c < 0 || c >= kNumClasses) return fail(LEV_ERR_ARG, "class out of range");
   if (v < -1 || v >= kNumPairVariants)
     return fail(LEV_ERR_ARG, "pair variant out of range (-1 turns pairs off)");
@@ -1871,6 +1951,7 @@ int lev_set_pair_variant(LevEngine *h, int32_t c, int32_t v) {
 }
 
 int lev_time_launches(LevEngine *h, float dt, int32_t n, float *ms_out) {
+  if (h) spec_drop(h);
   if (!h || !ms_out) return fail(LEV_ERR_ARG, "null argument");
   if (n < 1) return fail(LEV_ERR_ARG, "n must be >= 1");
   if (!std::isfinite(dt)) return fail(LEV_ERR_ARG, "dt is not finite");
@@ -1933,6 +2014,7 @@ int lev_class_info(const LevEngine *h, int32_t c, int32_t *ntiles,
 
 int lev_set_variant(LevEngine *h, int32_t c, int32_t v) {
   if (!h) return fail(LEV_ERR_ARG, "null handle");
+  spec_drop(h);
   if (c < 0 || c >= kNumClasses) return fail(LEV_ERR_ARG, "class out of range");
   if (v < 0 || v >= kNumVariants) return fail(LEV_ERR_ARG, "variant out of range");
   if (h->classes[c].variant != v) {
@@ -1983,6 +2065,7 @@ static int snapshot_copy(LevEngine *h, StateSnapshot &s, bool save) {
 int lev_autotune(LevEngine *h, float dt, int32_t trial_steps,
                  int32_t *variant_out, float *ms_out) {
   if (!h) return fail(LEV_ERR_ARG, "null handle");
+  spec_drop(h);
   if (trial_steps < 1) return fail(LEV_ERR_ARG, "trial_steps must be >= 1");
   if (!std::isfinite(dt)) return fail(LEV_ERR_ARG, "dt is not finite");
   DeviceScope ds(h->device);
@@ -2211,6 +2294,7 @@ int lev_hubs_create(LevHubs **out, int32_t num_hubs, const int32_t *hub_idx) {
 
 int lev_attach_hubs(LevEngine *h, int32_t net, LevHubs *m) {
   if (!h) return fail(LEV_ERR_ARG, "null handle");
+  spec_drop(h);
   DeviceScope ds(h->device);
   LEV_TRY_CUDA(cudaStreamSynchronize(h->stream));
   if (!m) {  // detach

@@ -148,6 +148,13 @@ struct StepArgs {
   int reverse;  // 1: CTAs walk the tile list backwards (alternating sweeps)
   float2 *pend;  // [nodes] (coupling sum, eps) of a half-done step (lev_pair.cuh)
   HubMonitor *hubs;  // observes hub phases after every step of hubs->net, or null
+  // speculative second step (lev_pair.cuh), or null: pair_kernel writes step
+  // t+1's new weights to w2 (SELL) and its predictor (theta_hat, omega_hat
+  // after step t+1) to thh2 / omh2, leaving the engine state exactly that
+  // after step t; finish_kernel moves thh2 / omh2 in
+  float *w2;
+  float *thh2;
+  float *omh2;
 };
 
 // ---------------------------------------------------------------------------

@@ -157,9 +157,10 @@ __device__ __forceinline__ int nxt_slot(int cur, int bsi) {
 //   DEEP = 1:   two stages: while group k0 computes, the gathers of group
 //               k0+U (whose col/delay words arrived during the previous
 //               group) and the stream loads of group k0+2U are in flight.
+// wo: where the second walk writes the new weights (wp: in place).
 template <int MATH, int U, int SECOND, int DEEP>
 __device__ __forceinline__ float row_walk(const uint32_t *__restrict__ cdp,
-                                          float *__restrict__ wp, int len, int deg,
+                                          float *wp, float *wo, int len, int deg,
                                           const float *__restrict__ ring, int base,
                                           int bsi, int Np, float th, float my_eps,
                                           float dt, const NetDesc &nd) {
@@ -207,7 +208,7 @@ __device__ __forceinline__ float row_walk(const uint32_t *__restrict__ cdp,
         if (!isfinite(w)) w = w_min;
         w = fmaxf(w_min, fminf(w_max, w));
         if (SECOND)
-          __stcs(wp + 32 * (k0 + u), w);
+          __stcs(wo + 32 * (k0 + u), w);
         else
           __stcg(wp + 32 * (k0 + u), w);
       }
@@ -302,19 +303,20 @@ __global__ void __launch_bounds__(kTile, MINB) pair_kernel(const StepArgs a) {
   const bool slice_live = slice_row0 < N;  // warp-uniform
   int len = 0;
   const uint32_t *cdp = nullptr;
-  float *wp = nullptr;
+  float *wp = nullptr, *wo = nullptr;
   if (slice_live) {
     const long long s = nd.slice_base + (slice_row0 >> 5);
     len = a.sl_len[s];
     const long long base = a.sl_off[s] + lane;
     cdp = a.sl_cd + base;
     wp = a.sl_w + base;
+    wo = (a.w2 ? a.w2 : a.sl_w) + base;
   }
 
   // ---- step t: edges (csr_physics_kernel, :126-165) -------------------------
   float sum0 = 0.0f;
   if (slice_live)
-    sum0 = row_walk<MATH, U, 0, DEEP>(cdp, wp, len, deg, ring, cur, bsi, Np, th, fabsf(eps),
+    sum0 = row_walk<MATH, U, 0, DEEP>(cdp, wp, wp, len, deg, ring, cur, bsi, Np, th, fabsf(eps),
                                       dt, nd);
 
   // ---- step t: integrate (integrate_and_reduce_kernel, :182-196) ------------
@@ -333,14 +335,21 @@ __global__ void __launch_bounds__(kTile, MINB) pair_kernel(const StepArgs a) {
     float diff = th1 - thh;
     diff = wrap_pm_pi(diff);
     eps1 = sinf(diff);
-    a.theta_hat[gi] = thh + dt * wh;
-    a.omega_hat[gi] = wh + nd.kappa_w * dt * eps1;
+    if (a.thh2) {  // speculative: the state stays that after step t
+      a.theta_hat[gi] = thh;
+      a.omega_hat[gi] = wh;
+      a.thh2[gi] = thh + dt * wh;
+      a.omh2[gi] = wh + nd.kappa_w * dt * eps1;
+    } else {
+      a.theta_hat[gi] = thh + dt * wh;
+      a.omega_hat[gi] = wh + nd.kappa_w * dt * eps1;
+    }
   }
 
   // ---- step t+1: edges; the integrate waits for g(t+1) (finish_kernel) ------
   float sum1 = 0.0f;
   if (slice_live)
-    sum1 = row_walk<MATH, U, 1, DEEP>(cdp, wp, len, deg, ring, nxt, bsi, Np, th1,
+    sum1 = row_walk<MATH, U, 1, DEEP>(cdp, wp, wo, len, deg, ring, nxt, bsi, Np, th1,
                                       fabsf(eps1), dt, nd);
   if (live) a.pend[gi] = make_float2(sum1, eps1);
 
@@ -406,6 +415,10 @@ __global__ void __launch_bounds__(kTile) finish_kernel(const StepArgs a, int nti
       if (!isfinite(x)) x = 0.0f;
       a.theta[gi] = x;
       a.ring[nd.ring_off + (long long)nxt * nd.Np + row] = x;
+      if (a.thh2) {  // the predictor of a speculative pair
+        a.theta_hat[gi] = a.thh2[gi];
+        a.omega_hat[gi] = a.omh2[gi];
+      }
       lev_sincos<MATH>(x, &my_sin[q], &my_cos[q]);
     }
   }

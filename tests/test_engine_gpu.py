@@ -258,6 +258,60 @@ def test_step_n_equals_repeated_step():
     assert a.step_count() == b.step_count() == 300
 
 
+@pytest.mark.parametrize("batch", [False, True])
+def test_speculative_single_steps_bit_identical(batch):
+    """Single steps run as speculative pairs (the pair kernel's second walk
+    into shadow buffers, finished by the next call): after every call the
+    engine state equals that of plain one-step blocks, bit for bit, with the
+    state read back and written (theta, weights, gain, controller,
+    parameters, dt) between calls."""
+    nets = [make_network(20_000, 16, 0.1, 30, seed=31)]
+    if batch:
+        nets += [make_network(3000, 12, 0.1, 20, seed=32)]
+
+    def make():
+        if batch:
+            return BatchEngine([n.as_dict() for n in nets])
+        return LeviathanEngine(*nets[0].engine_args())
+
+    a, b = make(), make()
+    for e in (a, b):
+        e.set_cluster_mode(False)
+        e.set_grid_mode(False)
+    assert all(c["enabled"] for c in a.pair_info() if c["eligible"])
+    rng = np.random.default_rng(5)
+    dt = DT
+    for k in range(40):
+        ra = a._step_all(dt)
+        rb = b._step_n_all(dt, 1)[0]
+        np.testing.assert_array_equal(ra, rb, err_msg=f"step {k}")
+        if k % 3 == 0:
+            sa, sb = _full_state(a), _full_state(b)
+            for key, want in sb.items():
+                np.testing.assert_array_equal(sa[key], want, err_msg=f"step {k}: {key}")
+        if k == 10:
+            for e in (a, b):
+                e._set_gain(0.7, 0)
+        if k == 14:
+            for e in (a, b):
+                e._set_ctrl(False, 0)
+        if k == 19:
+            th = rng.uniform(0, 2 * np.pi, a.total_nodes).astype(np.float32)
+            for e in (a, b):
+                e.set_all_theta(th)
+        if k == 25:
+            dt = 0.04
+        if k == 31:
+            for e in (a, b):
+                e._set_ctrl(True, 0)
+                e.set_params(0, eta=0.02) if batch else e.set_params(eta=0.02)
+    sa, sb = _full_state(a), _full_state(b)
+    for key, want in sb.items():
+        np.testing.assert_array_equal(sa[key], want, err_msg=key)
+    a.close()
+    b.close()
+
+
 def test_batch_equals_individual_engines():
     nets = [make_network(n, k, 0.1, md, seed=s, delay_lo=min(1, md))
             for n, k, md, s in [(700, 8, 10, 1), (2500, 20, 50, 2), (256, 4, 3, 3),
