@@ -263,18 +263,20 @@ def fp64_error_small():
 # ---------------------------------------------------------------------------
 # plain engine, small (N=1000, k=20): latency-bound, reported in us/step
 # ---------------------------------------------------------------------------
-def run_small(args):
+def _resident_run(net, steps, label):
+    """Steps of a network small enough for the cluster- or grid-resident
+    paths (autotuned against graph replay), CUDA events on the engine
+    stream.  Its working set is L2-resident, so the achieved figure is the
+    algorithmic bytes per step (17E + 36N + 4) over the step time, against L2
+    rather than HBM."""
     import torch
 
     from leviathan_v1_b200 import LeviathanEngine
-    from leviathan_v1_b200.graphs import config_small
 
-    net = config_small(0)
     e = LeviathanEngine(*net.engine_args())
-    e.autotune(DT, trial_steps=10)  # chooses the cluster path or graph replay
-    info = e.cluster_info()
+    e.autotune(DT, trial_steps=10)  # cluster, grid or graph replay
+    ci, gi = e.cluster_info(), e.grid_info()
     stream = torch.cuda.ExternalStream(e.stream_ptr)
-    steps = 500
     e.step_n_async(DT, steps)
     e.synchronize()
     ev0 = torch.cuda.Event(enable_timing=True)
@@ -285,12 +287,33 @@ def run_small(args):
     ev1.synchronize()
     ms = ev0.elapsed_time(ev1)
     e.close()
-    return {"workload": "Watts-Strogatz N=1000, k=20, p=0.1, delays U[1,50], 500 steps, "
-                        "controller on",
-            "N": net.N, "E": net.E, "steps": steps, "us_per_step": ms * 1e3 / steps,
-            "edge_updates_per_s": net.E * steps / (ms / 1e3),
-            "path": ("cluster-resident kernel, %d CTAs" % info["ctas"]) if info["enabled"]
-                    else "step kernel graph replay"}
+    if ci["enabled"]:
+        path = "cluster-resident kernel, %d CTAs" % ci["ctas"]
+    elif gi["enabled"]:
+        path = "grid-resident kernel, %d CTAs of %d rows" % (gi["ctas"], gi["rows_per_cta"])
+    else:
+        path = "step kernel graph replay"
+    alg = algorithmic_bytes(net.N, net.E)
+    step_s = ms / 1e3 / steps
+    return {"workload": label, "N": net.N, "E": net.E, "steps": steps,
+            "us_per_step": step_s * 1e6, "edge_updates_per_s": net.E / step_s,
+            "algorithmic_bytes_per_step": alg, "algorithmic_GBps": alg / step_s / 1e9,
+            "path": path}
+
+
+def run_small(args):
+    from leviathan_v1_b200.graphs import config_small
+
+    return _resident_run(config_small(0), 500, "Watts-Strogatz N=1000, k=20, p=0.1, "
+                         "delays U[1,50], 500 steps, controller on")
+
+
+def run_mid(args):
+    from leviathan_v1_b200.graphs import config_adjoint
+
+    return _resident_run(config_adjoint(0), 2000, "Watts-Strogatz N=1e4, k=20, p=0.1, "
+                         "delays U[1,50], 2000 steps, controller on (the adjoint "
+                         "configuration's plain engine, reference math)")
 
 
 # ---------------------------------------------------------------------------
@@ -601,6 +624,7 @@ def run_ours(args, rank, world, local):
         line["batched"] = run_batched(args, rank, world, value)
     if rank == 0:
         line["small"] = run_small(args)
+        line["mid"] = run_mid(args)
     if rank == 0 and not args.no_adjoint:
         line["adjoint"] = run_adjoint(args)
         line["reservoir"] = run_reservoir(args)
