@@ -3,6 +3,7 @@
     python -m leviathan_v1_b200.profile_cases step      [--N 1000000 --k 32 --steps 5]
     python -m leviathan_v1_b200.profile_cases cluster   [--N 1000 --k 20 --steps 200]
     python -m leviathan_v1_b200.profile_cases grid      [--N 10000 --k 20 --steps 200]
+    python -m leviathan_v1_b200.profile_cases batched   [--batch 128 --steps 20]
     python -m leviathan_v1_b200.profile_cases adjoint   [--N 200000 --k 32 --T 100]
     python -m leviathan_v1_b200.profile_cases adjgrid   [--N 10000 --k 20 --T 200]
     python -m leviathan_v1_b200.profile_cases reservoir [--N 20000 --batch 8 --T 60]
@@ -77,6 +78,28 @@ def case_grid(a):
     dt = time.perf_counter() - t
     e.close()
     return dict(case="grid", N=a.N, E=net.E, steps=a.steps, s=dt, grid=info)
+
+
+def case_batched(a):
+    """The first `batch` networks of the 512-network coupling sweep (N
+    log-uniform in [500, 5e4], k in {8, 16, 20, 32}, delays [1,50], K swept,
+    controller off), autotuned, then `steps` steps in step blocks."""
+    from .engine import BatchEngine
+    from .graphs import batch_specs, build_batch
+
+    specs = batch_specs(512, seed=0)[:a.batch]
+    nets, params = build_batch(specs)
+    e = BatchEngine([n.as_dict() for n in nets], params=params)
+    e.autotune(0.05, trial_steps=3)
+    e.step_n(0.05, 3)
+    _sync()
+    t = time.perf_counter()
+    e.step_n(0.05, a.steps)
+    dt = time.perf_counter() - t
+    out = dict(case="batched", networks=len(nets), N=sum(n.N for n in nets),
+               E=sum(n.E for n in nets), steps=a.steps, s=dt)
+    e.close()
+    return out
 
 
 def case_adjoint(a):
@@ -154,12 +177,14 @@ def case_e2e(a):
                 snapshot_s=t3 - t2, step_n_per_step_us=(t4 - t3) / a.steps * 1e6)
 
 
-CASES = dict(step=case_step, cluster=case_cluster, grid=case_grid, adjoint=case_adjoint,
+CASES = dict(step=case_step, cluster=case_cluster, grid=case_grid, batched=case_batched,
+             adjoint=case_adjoint,
              adjgrid=case_adjoint,
              reservoir=case_reservoir, e2e=case_e2e)
 DEFAULTS = dict(step=dict(N=1_000_000, k=32, max_delay=64, steps=5),
                 cluster=dict(N=1000, k=20, max_delay=50, steps=200),
                 grid=dict(N=10_000, k=20, max_delay=50, steps=200),
+                batched=dict(N=0, k=0, max_delay=50, batch=128, steps=20),
                 adjgrid=dict(N=10_000, k=20, max_delay=50, T=200),
                 adjoint=dict(N=200_000, k=32, max_delay=50, T=100),
                 reservoir=dict(N=20_000, k=20, max_delay=50, T=60, batch=8),
