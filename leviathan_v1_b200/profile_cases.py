@@ -3,7 +3,7 @@
     python -m leviathan_v1_b200.profile_cases step      [--N 1000000 --k 32 --steps 5]
     python -m leviathan_v1_b200.profile_cases cluster   [--N 1000 --k 20 --steps 200]
     python -m leviathan_v1_b200.profile_cases grid      [--N 10000 --k 20 --steps 200]
-    python -m leviathan_v1_b200.profile_cases batched   [--batch 128 --steps 20]
+    python -m leviathan_v1_b200.profile_cases batched   [--batch 128 --steps 20 --pair -1]
     python -m leviathan_v1_b200.profile_cases adjoint   [--N 200000 --k 32 --T 100]
     python -m leviathan_v1_b200.profile_cases adjgrid   [--N 10000 --k 20 --T 200]
     python -m leviathan_v1_b200.profile_cases reservoir [--N 20000 --batch 8 --T 60]
@@ -83,7 +83,9 @@ def case_grid(a):
 def case_batched(a):
     """The first `batch` networks of the 512-network coupling sweep (N
     log-uniform in [500, 5e4], k in {8, 16, 20, 32}, delays [1,50], K swept,
-    controller off), autotuned, then `steps` steps in step blocks."""
+    controller off), autotuned, then `steps` steps in step blocks.  `pair` >= 0
+    sets that two-steps-per-launch variant for every class after the
+    autotuner (under a profiler the autotuner's timings do not hold)."""
     from .engine import BatchEngine
     from .graphs import batch_specs, build_batch
 
@@ -91,13 +93,16 @@ def case_batched(a):
     nets, params = build_batch(specs)
     e = BatchEngine([n.as_dict() for n in nets], params=params)
     e.autotune(0.05, trial_steps=3)
+    if a.pair >= 0:
+        for c in range(3):
+            e.set_pair_variant(c, a.pair)
     e.step_n(0.05, 3)
     _sync()
     t = time.perf_counter()
     e.step_n(0.05, a.steps)
     dt = time.perf_counter() - t
     out = dict(case="batched", networks=len(nets), N=sum(n.N for n in nets),
-               E=sum(n.E for n in nets), steps=a.steps, s=dt)
+               E=sum(n.E for n in nets), steps=a.steps, s=dt, pair_info=e.pair_info())
     e.close()
     return out
 
@@ -184,7 +189,7 @@ CASES = dict(step=case_step, cluster=case_cluster, grid=case_grid, batched=case_
 DEFAULTS = dict(step=dict(N=1_000_000, k=32, max_delay=64, steps=5),
                 cluster=dict(N=1000, k=20, max_delay=50, steps=200),
                 grid=dict(N=10_000, k=20, max_delay=50, steps=200),
-                batched=dict(N=0, k=0, max_delay=50, batch=128, steps=20),
+                batched=dict(N=0, k=0, max_delay=50, batch=128, steps=20, pair=-1),
                 adjgrid=dict(N=10_000, k=20, max_delay=50, T=200),
                 adjoint=dict(N=200_000, k=32, max_delay=50, T=100),
                 reservoir=dict(N=20_000, k=20, max_delay=50, T=60, batch=8),
@@ -195,7 +200,8 @@ def main(argv=None):
     ap = argparse.ArgumentParser()
     ap.add_argument("case", choices=sorted(CASES))
     for name, typ in (("N", int), ("k", int), ("max_delay", int), ("steps", int),
-                      ("T", int), ("batch", int), ("segment", int), ("seed", int)):
+                      ("T", int), ("batch", int), ("segment", int), ("seed", int),
+                      ("pair", int)):
         ap.add_argument(f"--{name}", type=typ, default=None)
     a = ap.parse_args(argv)
     d = dict(DEFAULTS[a.case], segment=50, seed=0, case=a.case)
