@@ -136,7 +136,13 @@ int lev_net_shape(const LevEngine *h, int32_t net, int32_t *N, int64_t *E,
  * (leviathan_kernel.cu:391-438): predictor, delayed gather + coupling +
  * Hebbian update, integration + ring write, order parameter r, gain
  * controller.  r_out[num_nets] receives r of theta(t+1) per network
- * (may be NULL).  Synchronous, like the reference. */
+ * (may be NULL).  Synchronous, like the reference.  When every degree class
+ * takes two steps per launch, a call that starts a pair also computes the
+ * next step up to its integrate into shadow buffers (the engine state is
+ * exactly that after this step); the next call, with the same dt and no
+ * state-writing call in between, only finishes it.  Results are bitwise the
+ * same either way; the first such call allocates one more SELL weight array
+ * and two node arrays. */
 int lev_step(LevEngine *h, float dt, float *r_out);
 
 /* n steps of every network in one call; the step loop is replayed from a
