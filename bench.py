@@ -23,8 +23,10 @@ Metric: edge-updates/s = E x steps / elapsed.
   per-step figure of the whole launch sequence is in ``step_sequence``.
 * ``--impl reference`` runs the reference engine itself (its
   leviathan_kernel.cu built from the reference sources for sm_100a, and its
-  stock 86;90 build, in oracle/_ref) through its C ABI on the same GPU, the
-  same job as ``e2e`` (the reference has no CPU implementation of the path).
+  stock 86;90 build, in oracle/_ref) through its C ABI on the same GPU (the
+  reference has no CPU implementation of the path): ``value`` is K steps
+  timed with CUDA events on its stream after construction and warm-up,
+  ``e2e`` the same whole job as ours with the same bytes declared.
 Multi-GPU: the single network does not shard; ``--gpus N`` runs N
 independent replicas (one per rank, distinct seeds), weak scaling.
 """
@@ -197,6 +199,26 @@ def build_workload(seed):
                         WORKLOAD["max_delay"], seed)
 
 
+def bench_config(N, E):
+    """The workload description both arms print (identical dicts)."""
+    return {"workload": WORKLOAD_NAME, "N": N, "E": E,
+            "max_delay": WORKLOAD["max_delay"], "dt": DT,
+            "parallelism": "replicas (one network per GPU; a single network "
+                           "does not shard)",
+            "l2": "inputs (1.2 GB) larger than L2 (126 MB); no flush"}
+
+
+def h2d_bytes(N, E):
+    """Host->device bytes of one job: row_ptr, col_idx, delays, weights,
+    theta, theta_hat, omega."""
+    return (N + 1) * 4 + E * (4 + 1 + 4) + N * 4 * 3
+
+
+def d2h_bytes(N, K):
+    """Device->host bytes of one job: r of every step, final phases."""
+    return 4 * K + 4 * N
+
+
 def launches_per_job(K, pairs, block=256):
     """Kernel launches of K steps run as step blocks of `block` steps (one
     graph each): a reset of the r-history counter per block, then per two
@@ -217,26 +239,66 @@ def algorithmic_bytes(N, E):
     return 17 * E + 36 * N + 4
 
 
-def cpu_baseline(net, budget_s=20.0):
-    """FP64 NumPy oracle (oracle/oracle64.py) on the host: a bounded sample
-    of steps of the same network."""
+def _phase_errors(theta, theta64, r, r64):
+    from oracle64 import circular_distance
+
+    d = circular_distance(theta, theta64)
+    return {"max_wrapped_phase_rad": float(d.max()), "mean_wrapped_phase_rad": float(d.mean()),
+            "max_abs_r": float(np.abs(np.asarray(r, np.float64) - np.asarray(r64)).max())}
+
+
+def cpu_baseline_and_fp64_prefix(net, budget_s=20.0):
+    """FP64 NumPy oracle (oracle/oracle64.py) on the host over the first
+    steps of the bench network, as many as fit in about ``budget_s``
+    (at least 3): timed, it is the CPU baseline; its phases after those
+    steps, against the engine's after the same steps (both math modes),
+    state the FP64 error of the bench configuration over that prefix."""
     sys.path.insert(0, os.path.join(REPO, "oracle"))
     from oracle64 import OracleEngine
 
+    from leviathan_v1_b200 import LeviathanEngine
+
     o = OracleEngine(*net.engine_args())
     t0 = time.perf_counter()
-    o.step(DT)  # first step: warm caches, allocations
+    r64 = [o.step(DT)]
     first = time.perf_counter() - t0
-    n = max(1, min(50, int(budget_s / max(first, 1e-3))))
+    n = max(3, min(50, int(budget_s / max(first, 1e-3))))
     t0 = time.perf_counter()
-    for _ in range(n):
-        o.step(DT)
+    for _ in range(n - 1):
+        r64.append(o.step(DT))
     el = time.perf_counter() - t0
-    return {"value": net.E * n / el, "unit": "edge-updates/s", "cores": 1,
+    base = {"value": net.E * (n - 1) / el, "unit": "edge-updates/s", "cores": 1,
             "kind": "port",
-            "sample": f"{n} steps (after 1 warm-up step) of the bench network, "
-                      f"FP64 NumPy oracle, single-threaded NumPy, "
-                      f"{os.cpu_count()} host cores present"}
+            "sample": f"steps 2..{n} of the bench network (step 1 untimed), FP64 "
+                      f"NumPy oracle, single-threaded NumPy, {os.cpu_count()} host "
+                      f"cores present"}
+    errs = {"steps": n, "note": f"prefix of the run: the first {n} steps from the "
+                                f"bench's initial state"}
+    for mode in ("reference", "accurate"):
+        e = LeviathanEngine(*net.engine_args(), math_mode=mode)
+        r = e.step_n(DT, n)
+        errs[mode] = _phase_errors(e.get_theta(), o.theta, r, r64)
+        e.close()
+    return base, errs
+
+
+def fp64_error_batched_prefix(eng, nets, params, picks, steps=10):
+    """Error of sampled networks of a batched engine against the FP64
+    oracle over the next ``steps`` steps from the engine's current state
+    (a prefix; the engine must be at its initial state)."""
+    sys.path.insert(0, os.path.join(REPO, "oracle"))
+    from oracle64 import OracleEngine
+
+    r = eng.step_n(DT, steps)
+    out = {"steps": steps, "networks": []}
+    for i in picks:
+        o = OracleEngine(*nets[i].engine_args(), params=params[i])
+        r64 = o.run(DT, steps)
+        err = _phase_errors(eng.get_theta(i), o.theta, r[:, i], r64)
+        err.update(N=nets[i].N, E=nets[i].E, K=params[i]["g"])
+        out["networks"].append(err)
+    out["max_wrapped_phase_rad"] = max(x["max_wrapped_phase_rad"] for x in out["networks"])
+    return out
 
 
 def fp64_error_small():
@@ -333,7 +395,15 @@ def run_batched(args, rank, world, plain_value):
     E_local = sum(n.E for n in nets)
     N_local = sum(n.N for n in nets)
     eng = BatchEngine([n.as_dict() for n in nets], params=params)
-    tune = eng.autotune(DT, trial_steps=5)
+    tune = eng.autotune(DT, trial_steps=5)  # the state is restored afterwards
+    # FP64 error over a 10-step prefix of four sampled networks (K spread),
+    # from the initial state; the timing below continues from there
+    picks = [i for i in np.argsort([p["g"] for p in params])[[0, len(nets) // 3,
+                                                              2 * len(nets) // 3, -1]]]
+    picks = [int(i) for i in picks if nets[i].N <= 20_000] or [int(np.argmin([n.N for n in nets]))]
+    fp64 = fp64_error_batched_prefix(eng, nets, params, picks) if rank == 0 else None
+    if rank != 0:
+        eng.step_n(DT, 10)
     S = args.batched_steps
     eng.step_n_async(DT, max(args.warmup, 3))
     eng.synchronize()
@@ -352,7 +422,7 @@ def run_batched(args, rank, world, plain_value):
     N_tot = sum_over_ranks(N_local, world)
     value = E_tot * S / (ms / 1e3)
     # r(K) curve: sweep continues to 1000 steps in total, mean r of the last 100
-    done = 3 + S
+    done = 10 + max(args.warmup, 3) + S
     r = eng.step_n(DT, max(1000 - done, 100))
     curve = gather_results(mine, summarize_r(r, 100), len(specs))
     eng.close()
@@ -380,6 +450,7 @@ def run_batched(args, rank, world, plain_value):
             "autotune": {"chosen": tune["chosen"], "ms": tune["ms"],
                          "variants": tune["variants"]},
             "r_of_K_bins_0_to_4": r_of_K,
+            "fp64_error_prefix": fp64,
             "algorithmic_bytes_per_step": int(17 * E_tot + 36 * N_tot)}
 
 
@@ -541,8 +612,8 @@ def run_ours(args, rank, world, local):
     # end-to-end through the public API with host buffers: construction from
     # host arrays, K steps with r of every step returned to the host (the
     # block form used by LeviathanObservatory.run_baseline), final phases
-    h2d = (N + 1) * 4 + E * (4 + 1 + 4) + N * 4 * 3
-    d2h = 4 * K + 4 * N
+    h2d = h2d_bytes(N, E)
+    d2h = d2h_bytes(N, K)
     barrier(world)
     torch.cuda.synchronize()
     t0 = time.perf_counter()
@@ -599,10 +670,7 @@ def run_ours(args, rank, world, local):
         "n_gpus": world, "steps": K, "warmup": W, "ms_per_step": ms_max / K,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
         "dtype": "f32", "data": "synthetic (seeded Watts-Strogatz, seeded states)",
-        "config": {"workload": WORKLOAD_NAME, "N": N, "E": E,
-                   "max_delay": WORKLOAD["max_delay"], "dt": DT,
-                   "parallelism": f"replicas x{world} (single network does not shard)",
-                   "l2": "inputs (1.2 GB) larger than L2 (126 MB); no flush"},
+        "config": bench_config(N, E),
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak,
                      "unit": "GB/s", "frac": achieved / peak, "peak_kind": peak_kind,
                      "traffic": traffic, "kernel": kernel,
@@ -629,7 +697,8 @@ def run_ours(args, rank, world, local):
         line["adjoint"] = run_adjoint(args)
         line["reservoir"] = run_reservoir(args)
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        line["cpu_baseline"] = cpu_baseline(net, budget_s=args.cpu_budget)
+        line["cpu_baseline"], line["fp64_error_prefix"] = cpu_baseline_and_fp64_prefix(
+            net, budget_s=args.cpu_budget)
     if rank == 0 and not args.no_fp64_check:
         line["fp64_error_small_200_steps"] = fp64_error_small()
     if rank == 0:
@@ -640,6 +709,15 @@ def run_ours(args, rank, world, local):
 # reference engine (oracle/_ref, built from the reference sources)
 # ---------------------------------------------------------------------------
 def run_reference(args, rank, world, local):
+    """The reference engine, same network, same job, same GPU.
+
+    ``value``: after construction and W warm-up steps, K ``leviathan_step``
+    calls (each with its stock 4-byte r read-back, stream synchronisation and
+    host gain controller, leviathan_kernel.cu:391-438) timed with CUDA events
+    on the engine's own stream.  ``e2e``: construction from host arrays
+    (leviathan_init, :270-389), K steps and ``leviathan_get_theta`` (:440),
+    wall clock, with the host<->device bytes declared exactly as for this
+    repository's arm.  The faster of the two reference builds is reported."""
     if rank != 0:
         return
     import torch
@@ -648,50 +726,63 @@ def run_reference(args, rank, world, local):
     import refengine
 
     net = build_workload(seed=0)
+    N, E = net.N, net.E
     K, W = args.steps, args.warmup
-    results = {}
+    device, e2e_s, parts = {}, {}, {}
     for flavor in ("sm100a", "stock"):
         if not refengine.available(flavor):
             continue
-        # warm-up run (JIT of the stock build, allocations)
         ref = refengine.RefEngine(*net.engine_args(), flavor=flavor)
         for _ in range(W):
             ref.step(DT)
+        stream = torch.cuda.ExternalStream(ref.stream)
+        torch.cuda.synchronize()
+        ev0 = torch.cuda.Event(enable_timing=True)
+        ev1 = torch.cuda.Event(enable_timing=True)
+        ev0.record(stream)
+        for _ in range(K):
+            ref.step(DT)
+        ev1.record(stream)
+        ev1.synchronize()
+        device[flavor] = E * K / (ev0.elapsed_time(ev1) / 1e3)
         ref.close()
         torch.cuda.synchronize()
         t0 = time.perf_counter()
         ref = refengine.RefEngine(*net.engine_args(), flavor=flavor)
+        t1 = time.perf_counter()
         for _ in range(K):
             ref.step(DT)
+        t2 = time.perf_counter()
         ref.get_theta()
         torch.cuda.synchronize()
         el = time.perf_counter() - t0
+        parts[flavor] = {"construct_s": t1 - t0, "steps_s": t2 - t1,
+                         "get_theta_s": el - (t2 - t0)}
         ref.close()
-        results[flavor] = net.E * K / el
-    if not results:
+        e2e_s[flavor] = el
+    if not device:
         print(json.dumps({"impl": "reference", "unavailable":
                           "oracle/_ref reference build missing (make -C oracle)"}))
         return
-    best = max(results, key=results.get)
-    v = results[best]
+    best = max(device, key=device.get)
+    v = device[best]
     line = {
         "impl": "reference", "metric": "edge-updates/s", "value": v,
         "unit": "edge-updates/s", "n_gpus": 1, "steps": K, "warmup": W,
-        "ms_per_step": net.E / v * 1e3, "higher_is_better": True,
+        "ms_per_step": E / v * 1e3, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f32",
         "data": "synthetic (seeded Watts-Strogatz, seeded states)",
-        "config": {"workload": WORKLOAD_NAME, "N": net.N, "E": net.E,
-                   "max_delay": WORKLOAD["max_delay"], "dt": DT,
-                   "parallelism": "single GPU (rank 0)"},
-        "reference_builds": results, "reference_build_used": best,
-        "e2e": {"value": v, "unit": "edge-updates/s", "h2d_bytes_per_step": 0,
-                "d2h_bytes_per_step": 0},
-        "cpu_baseline": {"value": v, "unit": "edge-updates/s", "cores": 1,
-                         "kind": "reference",
-                         "sample": "the reference engine itself (leviathan_init + K x "
-                                   "leviathan_step + leviathan_get_theta) on the same "
-                                   "B200, one host thread; the reference implements "
-                                   "the path only in CUDA"},
+        "config": bench_config(N, E),
+        "timing": "value: CUDA events on the reference engine's stream around K "
+                  "leviathan_step calls after construction and W warm-up steps",
+        "reference_builds": {"device": device, "e2e_seconds": e2e_s},
+        "reference_build_used": best,
+        "e2e": {"value": E * K / e2e_s[best], "unit": "edge-updates/s",
+                "h2d_bytes_per_step": h2d_bytes(N, E) / K,
+                "d2h_bytes_per_step": d2h_bytes(N, K) / K,
+                "path": "leviathan_init(host arrays) + K x leviathan_step -> r "
+                        "+ leviathan_get_theta",
+                "seconds": e2e_s[best], "parts": parts[best]},
         "gpu_launches": 4 * K,
     }
     print(json.dumps(line), flush=True)

@@ -265,6 +265,18 @@ int lev_grid_info(const LevEngine *h, int32_t *eligible, int32_t *enabled, int32
                   int32_t *rows_per_cta, int64_t *smem_bytes, int32_t *eligible_rows_mask);
 int lev_set_grid_mode(LevEngine *h, int32_t enabled, int32_t rows_per_cta);
 
+/* Bound of the grid-barrier waits of the grid-resident step blocks (no
+ * reference counterpart).  limit_ns (1 us .. 60 s, default 2 s): longest
+ * time one wait may take before the kernel gives up, sets the error flag and
+ * returns.  extra_arrivals: 0 in normal use; a positive value makes every
+ * wait expect that many more arrivals than the grid makes, so the block's
+ * first wait runs out -- for tests of the timeout path, which then neither
+ * faults nor hangs the GPU.  After a timeout at the first wait every CTA has
+ * done the block's first step into its shared memory and one ring slot that
+ * no step of the restored state reads, and has written nothing else back:
+ * the engine keeps the state it had before the block. */
+int lev_set_grid_wait(LevEngine *h, uint64_t limit_ns, uint32_t extra_arrivals);
+
 /* Two steps per launch (no reference counterpart).  When no delay of the
  * engine is 0, step t+1's predictor and edge work need only the row's own
  * theta(t+1) and ring slots written before step t, so step blocks
@@ -276,8 +288,10 @@ int lev_set_grid_mode(LevEngine *h, int32_t enabled, int32_t rows_per_cta);
  * Results are bitwise those of one step per launch.  lev_autotune times the pair variants of each
  * degree class against its best one-step variant and keeps pairs only where
  * they are faster; pair_variant -1 means one step per launch for that class.
- * lev_step (single steps, and the reference ABI) always takes one step per
- * launch. */
+ * lev_step (single steps, and the reference ABI) uses the same pair launches
+ * as speculative single steps: the call that starts a pair leaves the state
+ * of its own step and keeps the next step's work in shadow buffers for the
+ * following call (see lev_step). */
 int lev_num_pair_variants(void);
 int lev_pair_variant_info(int32_t v, int32_t *unroll, int32_t *min_blocks,
                           int32_t *deep);
@@ -371,6 +385,8 @@ int lev_adj_grid_info(const LevAdjoint *a, int32_t *eligible, int32_t *enabled,
                       int32_t *rows_per_cta, int32_t *eligible_rows_mask, int32_t *paired);
 int lev_adj_set_grid_mode(LevAdjoint *a, int32_t enabled, int32_t rows_per_cta);
 int lev_adj_set_grid_pairing(LevAdjoint *a, int32_t enabled);
+/* Bound of the adjoint's grid-barrier waits, as lev_set_grid_wait. */
+int lev_adj_set_grid_wait(LevAdjoint *a, uint64_t limit_ns, uint32_t extra_arrivals);
 
 /* Self-test of the phase wraps (no reference counterpart; checks this
  * library's division-free evaluation of the wraps of
@@ -379,6 +395,66 @@ int lev_adj_set_grid_pairing(LevAdjoint *a, int32_t enabled);
  * division; *mismatch_pm / *mismatch_02 receive the number of inputs whose
  * results differ in any bit (0 expected). */
 int lev_selftest_wraps(uint64_t *mismatch_pm, uint64_t *mismatch_02);
+
+/* ------------------------------------------------------------------------ */
+/* One network split over several GPUs (halo engine)                         */
+/* ------------------------------------------------------------------------ */
+
+/* Replaces the reference's multi-GPU engine (multigpu_init / multigpu_step,
+ * leviathan_multigpu.cu:123-238, whose halo kernels :97-115 are never
+ * launched and whose step averages per-GPU |r| on the host) and the halo
+ * lists of its partitioner (python/partition.py:45-170, which drops every
+ * edge that crosses partitions, :121).
+ *
+ * The network's rows are cut into contiguous ranges of whole 256-row tiles;
+ * a partition engine holds one range ("own" rows, N of them, starting at
+ * global row 256 * tile_off_global) and ring columns for the n_halo other
+ * nodes its rows read ("halo" nodes).  Its CSR is the own rows' part of the
+ * network's CSR with columns renumbered: own node j -> j - 256 *
+ * tile_off_global, halo node -> N + its position in the partition's halo
+ * list; edge order within a row is kept, so every coupling sum is that of
+ * the single-GPU engine.  theta_halo[n_halo] are the halo nodes' phases
+ * (every ring slot of a halo column starts equal to them).  N_global and
+ * ntiles_global = ceil(N_global / 256) describe the whole network.  Every
+ * partition but the last owns a multiple of 256 rows.
+ *
+ * One step, all on the engine stream (lev_get_stream), device pointers:
+ *   lev_part_step_begin  predictor, edges, integrate and own ring columns;
+ *                        writes this partition's tile partials of
+ *                        (sum cos, sum sin) to partials[tile_off_global ..
+ *                        + own tiles) of a float2[ntiles_global] array;
+ *   (caller)             all-gather the partials of every partition into
+ *                        one float2[ntiles_global] array;
+ *   lev_part_step_end    r of the whole network from that array in the
+ *                        reference's order and the gain controller: every
+ *                        partition gets the same r and g, bitwise those of
+ *                        the single-GPU engine; r is also written to *r_dev
+ *                        (device, may be NULL);
+ *   lev_part_pack        out[k] = theta(t+1) of own node idx[k];
+ *   (caller)             send / receive to the peers;
+ *   lev_part_unpack      halo column idx[k] of the ring slot of theta(t+1)
+ *                        := in[k], before the next step.
+ * Indices out of range are skipped.  lev_set_theta / lev_get_theta work on
+ * the own nodes; lev_part_fill_halo(theta_halo host) refills every ring slot
+ * of the halo columns (the rest of set_theta).  lev_step, lev_step_n,
+ * autotuning, hub monitors and the adjoint are refused (LEV_ERR_STATE). */
+int lev_part_create(LevEngine **out, int32_t N, int32_t n_halo, int32_t max_delay,
+                    const int32_t *row_ptr, const int32_t *col_idx,
+                    const uint8_t *delays, const float *weights,
+                    const float *theta, const float *theta_hat,
+                    const float *omega, const float *theta_halo,
+                    int32_t N_global, int32_t tile_off_global,
+                    int32_t ntiles_global, const LevParams *params,
+                    int32_t math_mode);
+int lev_part_info(const LevEngine *h, int32_t *n_halo, int32_t *N_global,
+                  int32_t *tile_off_global, int32_t *ntiles_global);
+int lev_part_step_begin(LevEngine *h, float dt, void *partials_dev);
+int lev_part_step_end(LevEngine *h, float dt, const void *partials_all_dev,
+                      float *r_dev);
+int lev_part_pack(LevEngine *h, const int32_t *idx_dev, int32_t n, float *out_dev);
+int lev_part_unpack(LevEngine *h, const int32_t *idx_dev, int32_t n,
+                    const float *in_dev);
+int lev_part_fill_halo(LevEngine *h, const float *theta_halo);
 
 /* ------------------------------------------------------------------------ */
 /* Allocation-free step                                                      */
@@ -397,10 +473,14 @@ int lev_selftest_wraps(uint64_t *mismatch_pm, uint64_t *mismatch_02);
  * legacy default stream); returns after the launch.  Same arithmetic and
  * results as lev_step.  All array arguments are DEVICE pointers on the
  * current device:
- *   row_ptr[N+1], col_idx[E], delays[E]   CSR topology (must be valid: E =
- *                                         row_ptr[N], col < N, delay <=
- *                                         max_delay; out-of-range edges are
- *                                         skipped, not read)
+ *   row_ptr[N+1], col_idx[E], delays[E]   CSR topology: E = row_ptr[N],
+ *                                         col < N, delay <= max_delay.  No
+ *                                         error is raised for an edge whose
+ *                                         col or delay is out of range: it is
+ *                                         skipped (no ring read, nothing added
+ *                                         to the coupling sum, its weight left
+ *                                         unchanged).  Every pointer must be
+ *                                         non-NULL, also when E = 0.
  *   weights[E], theta[N], theta_hat[N], omega_hat[N]   state, updated
  *   omega[N]                              natural frequencies
  *   ring[(max_delay+2)*N]                 delay ring, slot-major: slot s of

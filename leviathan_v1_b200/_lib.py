@@ -132,10 +132,22 @@ PROTOTYPES = {
                                     C.POINTER(_i32), C.POINTER(_i32)]),
     "lev_adj_set_grid_mode": (C.c_int, [_P, _i32, _i32]),
     "lev_adj_set_grid_pairing": (C.c_int, [_P, _i32]),
+    "lev_adj_set_grid_wait": (C.c_int, [_P, C.c_uint64, C.c_uint32]),
+    "lev_set_grid_wait": (C.c_int, [_P, C.c_uint64, C.c_uint32]),
     "lev_selftest_wraps":(C.c_int, [C.POINTER(C.c_uint64), C.POINTER(C.c_uint64)]),
     "lev_step_noalloc":(C.c_int, [_i32, _i32, _i64, _P, _P, _P, _P, _P, _P, _P,
                                    _P, _P, _P, _P, C.POINTER(LevParams), _f32,
                                    _i32, _P]),
+    "lev_part_create": (C.c_int, [C.POINTER(_P), _i32, _i32, _i32, _P, _P, _P, _P, _P,
+                                  _P, _P, _P, _i32, _i32, _i32, C.POINTER(LevParams),
+                                  _i32]),
+    "lev_part_info": (C.c_int, [_P, C.POINTER(_i32), C.POINTER(_i32), C.POINTER(_i32),
+                                C.POINTER(_i32)]),
+    "lev_part_step_begin": (C.c_int, [_P, _f32, _P]),
+    "lev_part_step_end": (C.c_int, [_P, _f32, _P, _P]),
+    "lev_part_pack": (C.c_int, [_P, _P, _i32, _P]),
+    "lev_part_unpack": (C.c_int, [_P, _P, _i32, _P]),
+    "lev_part_fill_halo": (C.c_int, [_P, _P]),
     "lev_gen_ws": (C.c_int, [_i32, _i32, C.c_double, C.c_uint64, _i32, _i32, _f32,
                              _f32, _f32, _f32, _P, _P, _P, _P, _P, _P]),
     "lev_hubs_create": (C.c_int, [C.POINTER(_P), _i32, _P]),

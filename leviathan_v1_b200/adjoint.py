@@ -75,6 +75,11 @@ class Adjoint:
     def set_grid_mode(self, enabled: bool, rows_per_cta: int = 0) -> None:
         check(self.lib.lev_adj_set_grid_mode(self._h, 1 if enabled else 0, int(rows_per_cta)))
 
+    def set_grid_wait(self, limit_ns: int = 2_000_000_000, extra_arrivals: int = 0) -> None:
+        """Bound of the grid-barrier waits of the segments (default 2 s);
+        ``extra_arrivals`` > 0 makes every wait run out (tests)."""
+        check(self.lib.lev_adj_set_grid_wait(self._h, int(limit_ns), int(extra_arrivals)))
+
     def set_grid_pairing(self, enabled: bool) -> None:
         """Recompute segment k-1 and reverse segment k in one paired launch
         (when eligible), or in launches of their own."""

@@ -56,6 +56,7 @@ struct AdjGridFwdArgs {
   float2 *wsum;        // [2][nwarps]
   unsigned *bar;
   int *err;
+  GridWait wait;  // bound of the barrier waits
   // the segment's checkpoint (theta, theta_hat, omega_hat, SELL weights, the
   // last max_delay+1 ring slots as [m][N], g): ck_mode 1 writes it from the
   // initial state (forward pass); 2 takes the initial state from it and
@@ -195,7 +196,7 @@ __device__ __forceinline__ void adj_grid_fwd_body(const AdjGridFwdArgs &a, const
       for (int m = q; m <= nd.max_delay; m += LPR)
         __stcg(ring_w + (long long)(nd.max_delay - m) * Np + row, a.ck_ring[(long long)m * N + row]);
     grid_arrive(a.bar);
-    if (!grid_wait(a.bar, G, a.err, &s_ok)) return;
+    if (!grid_wait(a.bar, G, a.err, &s_ok, a.wait)) return;
     base = G;
   }
 
@@ -231,7 +232,7 @@ __device__ __forceinline__ void adj_grid_fwd_body(const AdjGridFwdArgs &a, const
   bool ok = true;
   for (; step < a.n_steps; ++step) {
     if (step > 0 && !a.early) {
-      if (!(ok = grid_wait(a.bar, base + (unsigned)step * G, a.err, &s_ok))) break;
+      if (!(ok = grid_wait(a.bar, base + (unsigned)step * G, a.err, &s_ok, a.wait))) break;
       stage_sums(step - 1);
     }
     // ---- predictor (row's first lane) --------------------------------------
@@ -301,7 +302,7 @@ __device__ __forceinline__ void adj_grid_fwd_body(const AdjGridFwdArgs &a, const
     }
     if (step > 0) {
       if (a.early) {
-        if (!(ok = grid_wait(a.bar, base + (unsigned)step * G, a.err, &s_ok))) break;
+        if (!(ok = grid_wait(a.bar, base + (unsigned)step * G, a.err, &s_ok, a.wait))) break;
         stage_sums(step - 1);
       }
       reduce_prev(step);
@@ -353,7 +354,7 @@ __device__ __forceinline__ void adj_grid_fwd_body(const AdjGridFwdArgs &a, const
     grid_arrive(a.bar);
   }
   if (ok && a.n_steps > 0 && cta == 0)
-    ok = grid_wait(a.bar, base + (unsigned)a.n_steps * G, a.err, &s_ok);
+    ok = grid_wait(a.bar, base + (unsigned)a.n_steps * G, a.err, &s_ok, a.wait);
   if (!ok) return;
   if (a.n_steps > 0 && cta == 0 && warp == 0) {
     const float2 *src = a.wsum + ((a.n_steps - 1) & 1) * nwarps;
@@ -404,6 +405,7 @@ struct AdjGridBwdArgs {
   float *lgp;            // [2][group CTAs rounded up to 4] per-CTA lam_g parts
   unsigned *bar;
   int *err;
+  GridWait wait;  // bound of the barrier waits
   int early;             // no delay is 0: slot s+1 is complete one barrier earlier
   long long SL;
   long long seg_start;
@@ -566,7 +568,7 @@ __device__ __forceinline__ void adj_grid_bwd_body(const AdjGridBwdArgs &a, const
     const float dldr = a.dLdr ? a.dLdr[s] : 0.0f;
     // lam_g(s+1): the parts of reverse step s+1, after its barrier
     if (k > 0) {
-      if (!(ok = grid_wait(a.bar, (unsigned)k * G, a.err, &s_ok))) break;
+      if (!(ok = grid_wait(a.bar, (unsigned)k * G, a.err, &s_ok, a.wait))) break;
       fold_parts(k - 1);
       __syncthreads();
       lamg = s_lg;
@@ -649,7 +651,7 @@ __device__ __forceinline__ void adj_grid_bwd_body(const AdjGridBwdArgs &a, const
     grid_arrive(a.bar);
   }
   if (ok && a.n_steps > 0 && cta == 0) {
-    ok = grid_wait(a.bar, (unsigned)a.n_steps * G, a.err, &s_ok);
+    ok = grid_wait(a.bar, (unsigned)a.n_steps * G, a.err, &s_ok, a.wait);
     if (ok) {
       fold_parts(a.n_steps - 1);
       if (tid == 0) a.lam_g[0] = s_lg;

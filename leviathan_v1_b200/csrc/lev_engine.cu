@@ -25,6 +25,7 @@
 #include "lev_pair.cuh"
 #include "lev_cluster.cuh"
 #include "lev_grid.cuh"  // uses cluster_sums from lev_cluster.cuh
+#include "lev_part.cuh"
 
 namespace lev {
 
@@ -222,6 +223,15 @@ struct LevEngine {
   float2 *d_gwsum = nullptr;  // [2][grid_nwarps]
   unsigned *d_gbar = nullptr;
   int *h_gerr = nullptr, *d_gerr = nullptr;  // barrier timeout flag (mapped)
+  GridWait grid_wait = {kGridWaitNs, 0u, 0u};  // bound of the barrier waits
+
+  // partition of a network split over GPUs (lev_part.cuh, lev_part_*): own
+  // rows stepped here, halo phases in ring columns N .. N + part_halo - 1
+  bool part = false;
+  int part_halo = 0;
+  int part_N_global = 0;
+  int part_tile_off = 0;      // first global tile of the partition
+  int part_ntiles_global = 0;
 };
 
 struct LeviathanHandle {
@@ -739,6 +749,7 @@ int launch_grid(LevEngine *h, float dt, int len) {
   ga.bar = h->d_gbar;
   ga.early = h->pair_ok ? 1 : 0;  // no delay is 0
   ga.err = h->d_gerr;
+  ga.wait = h->grid_wait;
   ga.r_hist = h->d_rhist;
   ga.r_cap = h->block_len;
   ga.n_steps = len;
@@ -973,13 +984,42 @@ cudaError_t upload(void *dst, const void *src, size_t bytes, cudaStream_t s) {
   return (cudaError_t)failed.load();
 }
 
+// Every ring slot of halo columns N .. N + n_ext - 1 of network 0 := the
+// given host phases (the partition's part of init_buffer_kernel,
+// leviathan_kernel.cu:79-90).  Synchronous.
+int fill_ext_columns(LevEngine *h, int n_ext, const float *theta_ext) {
+  const NetDesc &nd = h->h_nets[0];
+  float *d_tmp = nullptr;
+  LEV_TRY_CUDA(cudaMalloc(reinterpret_cast<void **>(&d_tmp), sizeof(float) * n_ext));
+  cudaError_t e = cudaMemcpyAsync(d_tmp, theta_ext, sizeof(float) * n_ext,
+                                  cudaMemcpyHostToDevice, h->stream);
+  if (e == cudaSuccess) {
+    const long long total = (long long)nd.bsi * n_ext;
+    int blocks = (int)std::min<long long>((total + 255) / 256, 148LL * 16);
+    ring_fill_kernel<<<blocks, 256, 0, h->stream>>>(
+        d_tmp, h->d_ring + nd.ring_off + nd.N, n_ext, nd.Np, nd.bsi);
+    e = cudaGetLastError();
+  }
+  if (e == cudaSuccess) e = cudaStreamSynchronize(h->stream);
+  cudaFree(d_tmp);
+  if (e != cudaSuccess)
+    return fail(LEV_ERR_CUDA, std::string("halo ring fill: ") + cudaGetErrorString(e));
+  return LEV_OK;
+}
+
 int create_impl(LevEngine **out, int num_nets, const int32_t *Ns,
                 const int32_t *mds, const int32_t *rp_cat,
                 const int32_t *col_cat, const uint8_t *d_cat,
                 const float *w_cat, const float *th_cat,
                 const float *thh_cat, const float *om_cat,
-                const LevParams *params, int math_mode) {
+                const LevParams *params, int math_mode, int n_ext = 0,
+                const float *theta_ext = nullptr) {
+  // n_ext > 0 (one network only): ring columns N .. N + n_ext - 1 hold the
+  // phases of halo nodes of a partition (lev_part.cuh), initially theta_ext;
+  // col_idx may then address them
   if (!out) return fail(LEV_ERR_ARG, "out is null");
+  if (n_ext < 0 || (n_ext > 0 && (num_nets != 1 || !theta_ext)))
+    return fail(LEV_ERR_ARG, "halo columns need one network and their phases");
   *out = nullptr;
   if (num_nets < 1) return fail(LEV_ERR_ARG, "num_nets must be >= 1");
   if (!Ns || !mds || !rp_cat || !th_cat || !thh_cat || !om_cat)
@@ -1035,7 +1075,11 @@ int create_impl(LevEngine **out, int num_nets, const int32_t *Ns,
     d.ring_off = ring_off;
     d.rp_off = rp_off;
     d.N = N;
-    d.Np = (N + 31) / 32 * 32;
+    if ((long long)N + n_ext >= (1LL << 24)) {
+      delete h;
+      return fail(LEV_ERR_ARG, "N plus halo nodes must be below 2^24");
+    }
+    d.Np = (N + n_ext + 31) / 32 * 32;
     d.bsi = md + 2;
     d.max_delay = md;
     d.ntiles = (N + kTile - 1) / kTile;
@@ -1258,7 +1302,7 @@ int create_impl(LevEngine **out, int num_nets, const int32_t *Ns,
       if (h->net_E[n] == 0) continue;
       int blocks = (int)std::min<long long>((d.N + 255) / 256, 148LL * 16);
       sell_convert_kernel<<<blocks, 256, 0, h->stream>>>(
-          0, h->d_row_ptr + d.rp_off, d.N, d.slice_base, h->d_sl_off,
+          0, h->d_row_ptr + d.rp_off, d.N, d.N + n_ext, d.slice_base, h->d_sl_off,
           d_tcol + d.edge_off, d_tmp + d.edge_off, d_tw + d.edge_off,
           h->d_sl_cd, h->d_sl_w, d.max_delay, d_err);
     }
@@ -1299,6 +1343,14 @@ int create_impl(LevEngine **out, int num_nets, const int32_t *Ns,
   }
   for (int n = 0; n < num_nets; ++n) {
     int r2 = launch_fill(h, n);
+    if (r2 != LEV_OK) {
+      std::string msg = g_last_error;
+      free_engine(h);
+      return fail(r2, msg);
+    }
+  }
+  if (n_ext > 0) {
+    int r2 = fill_ext_columns(h, n_ext, theta_ext);
     if (r2 != LEV_OK) {
       std::string msg = g_last_error;
       free_engine(h);
@@ -1407,6 +1459,7 @@ int lev_net_shape(const LevEngine *h, int32_t net, int32_t *N, int64_t *E,
 
 int lev_step(LevEngine *h, float dt, float *r_out) {
   if (!h) return fail(LEV_ERR_ARG, "null handle");
+  if (h->part) return fail(LEV_ERR_STATE, "partition engine: step with lev_part_step_begin / lev_part_step_end");
   if (!std::isfinite(dt)) return fail(LEV_ERR_ARG, "dt is not finite");
   DeviceScope ds(h->device);
   StepArgs a = make_args(h, dt, nullptr, 0, h->d_rmap);
@@ -1462,6 +1515,7 @@ int lev_step(LevEngine *h, float dt, float *r_out) {
 
 int lev_step_n(LevEngine *h, float dt, int32_t n, float *r_out) {
   if (!h) return fail(LEV_ERR_ARG, "null handle");
+  if (h->part) return fail(LEV_ERR_STATE, "partition engine: step with lev_part_step_begin / lev_part_step_end");
   if (n < 0) return fail(LEV_ERR_ARG, "n must be >= 0");
   if (!std::isfinite(dt)) return fail(LEV_ERR_ARG, "dt is not finite");
   if (n == 0) return LEV_OK;
@@ -1491,6 +1545,7 @@ int lev_step_n(LevEngine *h, float dt, int32_t n, float *r_out) {
 
 int lev_step_n_async(LevEngine *h, float dt, int32_t n) {
   if (!h) return fail(LEV_ERR_ARG, "null handle");
+  if (h->part) return fail(LEV_ERR_STATE, "partition engine: step with lev_part_step_begin / lev_part_step_end");
   if (n < 0) return fail(LEV_ERR_ARG, "n must be >= 0");
   if (!std::isfinite(dt)) return fail(LEV_ERR_ARG, "dt is not finite");
   DeviceScope ds(h->device);
@@ -1574,7 +1629,7 @@ static int convert_weights(LevEngine *h, float *d_csr, int mode) {
     if (h->net_E[n] == 0) continue;
     int blocks = (int)std::min<long long>((d.N + 255) / 256, 148LL * 16);
     sell_convert_kernel<<<blocks, 256, 0, h->stream>>>(
-        mode, h->d_row_ptr + d.rp_off, d.N, d.slice_base, h->d_sl_off,
+        mode, h->d_row_ptr + d.rp_off, d.N, d.N, d.slice_base, h->d_sl_off,
         nullptr, nullptr, d_csr + d.edge_off, h->d_sl_cd, h->d_sl_w,
         d.max_delay, nullptr);
   }
@@ -1897,6 +1952,22 @@ int lev_set_grid_mode(LevEngine *h, int32_t enabled, int32_t rows_per_cta) {
   return LEV_OK;
 }
 
+static int check_wait_args(uint64_t limit_ns, uint32_t extra) {
+  if (limit_ns < 1000ull || limit_ns > 60000000000ull)
+    return fail(LEV_ERR_ARG, "limit_ns must be in [1 us, 60 s]");
+  if (extra > 1024u) return fail(LEV_ERR_ARG, "extra_arrivals must be <= 1024");
+  return LEV_OK;
+}
+
+int lev_set_grid_wait(LevEngine *h, uint64_t limit_ns, uint32_t extra_arrivals) {
+  if (!h) return fail(LEV_ERR_ARG, "null handle");
+  int rc = check_wait_args(limit_ns, extra_arrivals);
+  if (rc != LEV_OK) return rc;
+  h->grid_wait.ns = limit_ns;
+  h->grid_wait.extra = extra_arrivals;
+  return LEV_OK;
+}
+
 int lev_num_variants(void) { return kNumVariants; }
 
 int lev_num_pair_variants(void) { return kNumPairVariants; }
@@ -1953,6 +2024,7 @@ int lev_set_pair_variant(LevEngine *h, int32_t c, int32_t v) {
 int lev_time_launches(LevEngine *h, float dt, int32_t n, float *ms_out) {
   if (h) spec_drop(h);
   if (!h || !ms_out) return fail(LEV_ERR_ARG, "null argument");
+  if (h->part) return fail(LEV_ERR_STATE, "partition engine: not supported");
   if (n < 1) return fail(LEV_ERR_ARG, "n must be >= 1");
   if (!std::isfinite(dt)) return fail(LEV_ERR_ARG, "dt is not finite");
   DeviceScope ds(h->device);
@@ -2065,6 +2137,7 @@ static int snapshot_copy(LevEngine *h, StateSnapshot &s, bool save) {
 int lev_autotune(LevEngine *h, float dt, int32_t trial_steps,
                  int32_t *variant_out, float *ms_out) {
   if (!h) return fail(LEV_ERR_ARG, "null handle");
+  if (h->part) return fail(LEV_ERR_STATE, "partition engine: not supported");
   spec_drop(h);
   if (trial_steps < 1) return fail(LEV_ERR_ARG, "trial_steps must be >= 1");
   if (!std::isfinite(dt)) return fail(LEV_ERR_ARG, "dt is not finite");
@@ -2294,6 +2367,7 @@ int lev_hubs_create(LevHubs **out, int32_t num_hubs, const int32_t *hub_idx) {
 
 int lev_attach_hubs(LevEngine *h, int32_t net, LevHubs *m) {
   if (!h) return fail(LEV_ERR_ARG, "null handle");
+  if (h->part) return fail(LEV_ERR_STATE, "partition engine: not supported");
   spec_drop(h);
   DeviceScope ds(h->device);
   LEV_TRY_CUDA(cudaStreamSynchronize(h->stream));
@@ -2663,6 +2737,7 @@ struct LevAdjoint {
   float *g_lgp = nullptr;
   unsigned *g_bar = nullptr;
   int *h_gerr = nullptr, *d_gerr = nullptr;
+  GridWait grid_wait = {kGridWaitNs, 0u, 0u};  // bound of the barrier waits
 };
 
 namespace {
@@ -2929,6 +3004,7 @@ void adj_grid_fill_fwd(LevAdjoint *a, AdjGridFwdArgs &f, int n) {
   f.wsum = a->g_wsum;
   f.bar = a->g_bar;
   f.err = a->d_gerr;
+  f.wait = a->grid_wait;
   f.SL = a->SL;
   f.early = e->pair_ok ? 1 : 0;  // no delay is 0
   f.nwarps = a->g_nwarps;
@@ -2976,6 +3052,7 @@ void adj_grid_fill_bwd(LevAdjoint *a, AdjGridBwdArgs &b) {
   b.lgp = a->g_lgp;
   b.bar = a->g_bar;
   b.err = a->d_gerr;
+  b.wait = a->grid_wait;
   b.early = e->pair_ok ? 1 : 0;  // no delay is 0
   b.SL = a->SL;
   b.edge_cap = a->g_cap[ri];
@@ -3036,6 +3113,7 @@ int lev_adj_create(LevAdjoint **out, LevEngine *e, int32_t segment,
                    int32_t max_steps) {
   if (!out || !e) return fail(LEV_ERR_ARG, "null argument");
   *out = nullptr;
+  if (e->part) return fail(LEV_ERR_STATE, "partition engine: not supported");
   if (segment < 1 || max_steps < 1)
     return fail(LEV_ERR_ARG, "segment and max_steps must be >= 1");
   DeviceScope ds(e->device);
@@ -3190,7 +3268,7 @@ int lev_adj_forward(LevAdjoint *a, float dt, int32_t T, const float *omega,
     if (e->net_E[n] == 0) continue;
     int blocks = (int)std::min<long long>((d.N + 255) / 256, 148LL * 16);
     sell_convert_kernel<<<blocks, 256, 0, s>>>(
-        1, e->d_row_ptr + d.rp_off, d.N, d.slice_base, e->d_sl_off, nullptr,
+        1, e->d_row_ptr + d.rp_off, d.N, d.N, d.slice_base, e->d_sl_off, nullptr,
         nullptr, const_cast<float *>(w0_csr) + d.edge_off, e->d_sl_cd, a->w,
         d.max_delay, nullptr);
     const long long total = (long long)d.bsi * d.N;
@@ -3496,7 +3574,7 @@ int lev_adj_backward(LevAdjoint *a, const float *dLdr, const float *dLdtheta,
       if (e->net_E[n] == 0) continue;
       int blocks = (int)std::min<long long>((d.N + 255) / 256, 148LL * 16);
       sell_convert_kernel<<<blocks, 256, 0, s>>>(
-          2, e->d_row_ptr + d.rp_off, d.N, d.slice_base, e->d_sl_off, nullptr, nullptr,
+          2, e->d_row_ptr + d.rp_off, d.N, d.N, d.slice_base, e->d_sl_off, nullptr, nullptr,
           grad_w0_csr + d.edge_off, e->d_sl_cd, a->lam_w, d.max_delay, nullptr);
     }
   }
@@ -3523,6 +3601,15 @@ int lev_adj_grid_info(const LevAdjoint *a, int32_t *eligible, int32_t *enabled,
       if (a->gR_ok[i]) m |= kGridRs[i];
     *eligible_rows_mask = m;
   }
+  return LEV_OK;
+}
+
+int lev_adj_set_grid_wait(LevAdjoint *a, uint64_t limit_ns, uint32_t extra_arrivals) {
+  if (!a) return fail(LEV_ERR_ARG, "null handle");
+  int rc = check_wait_args(limit_ns, extra_arrivals);
+  if (rc != LEV_OK) return rc;
+  a->grid_wait.ns = limit_ns;
+  a->grid_wait.extra = extra_arrivals;
   return LEV_OK;
 }
 
@@ -3582,6 +3669,146 @@ int lev_adj_grad_theta0(LevAdjoint *a, float *grad_theta0) {
                                cudaMemcpyDeviceToDevice, a->e->stream));
   LEV_TRY_CUDA(cudaStreamSynchronize(a->e->stream));
   return LEV_OK;
+}
+
+}  // extern "C"
+
+// ===========================================================================
+// Partition of a network split over GPUs (lev_part.cuh)
+// ===========================================================================
+extern "C" {
+
+int lev_part_create(LevEngine **out, int32_t N, int32_t n_halo, int32_t max_delay,
+                    const int32_t *row_ptr, const int32_t *col_idx,
+                    const uint8_t *delays, const float *weights,
+                    const float *theta, const float *theta_hat,
+                    const float *omega, const float *theta_halo,
+                    int32_t N_global, int32_t tile_off_global,
+                    int32_t ntiles_global, const LevParams *params,
+                    int32_t math_mode) {
+  if (!out) return fail(LEV_ERR_ARG, "out is null");
+  *out = nullptr;
+  if (n_halo < 0) return fail(LEV_ERR_ARG, "n_halo must be >= 0");
+  if (n_halo > 0 && !theta_halo) return fail(LEV_ERR_ARG, "theta_halo is null");
+  if (N < 1 || N_global < N || tile_off_global < 0 || ntiles_global < 1 ||
+      (long long)tile_off_global * kTile + N > (long long)N_global ||
+      ntiles_global != (N_global + kTile - 1) / kTile)
+    return fail(LEV_ERR_ARG,
+                "partition: need 1 <= N, rows [256 * tile_off_global, + N) inside "
+                "N_global, ntiles_global = ceil(N_global / 256)");
+  if ((long long)tile_off_global * kTile + N < (long long)N_global && N % kTile != 0)
+    return fail(LEV_ERR_ARG, "partition: every partition but the last must own whole "
+                             "256-row tiles");
+  // a halo column that no edge reads is allowed (its phases are just kept)
+  LevEngine *h = nullptr;
+  int rc = create_impl(&h, 1, &N, &max_delay, row_ptr, col_idx, delays, weights,
+                       theta, theta_hat, omega, params, math_mode, n_halo,
+                       theta_halo);
+  if (rc != LEV_OK) return rc;
+  DeviceScope ds(h->device);
+  h->part = true;
+  h->part_halo = n_halo;
+  h->part_N_global = N_global;
+  h->part_tile_off = tile_off_global;
+  h->part_ntiles_global = ntiles_global;
+  // one step per launch with a host-driven reduction: none of the block paths
+  h->pair_ok = false;
+  h->use_pairs = false;
+  h->cluster_ok = false;
+  h->use_cluster = false;
+  h->grid_ok = false;
+  h->use_grid = false;
+  h->h_nets[0].dist = 1;
+  h->h_nets[0].part_off = tile_off_global;
+  cudaError_t e = cudaMemcpyAsync(h->d_nets, h->h_nets.data(), sizeof(NetDesc),
+                                  cudaMemcpyHostToDevice, h->stream);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(h->stream);
+  if (e != cudaSuccess) {
+    free_engine(h);
+    return fail(LEV_ERR_CUDA, std::string("partition set-up: ") + cudaGetErrorString(e));
+  }
+  *out = h;
+  return LEV_OK;
+}
+
+static int part_check(LevEngine *h) {
+  if (!h) return fail(LEV_ERR_ARG, "null handle");
+  if (!h->part) return fail(LEV_ERR_STATE, "not a partition engine (lev_part_create)");
+  return LEV_OK;
+}
+
+int lev_part_info(const LevEngine *h, int32_t *n_halo, int32_t *N_global,
+                  int32_t *tile_off_global, int32_t *ntiles_global) {
+  if (!h) return fail(LEV_ERR_ARG, "null handle");
+  if (n_halo) *n_halo = h->part ? h->part_halo : 0;
+  if (N_global) *N_global = h->part ? h->part_N_global : (int32_t)h->total_nodes;
+  if (tile_off_global) *tile_off_global = h->part ? h->part_tile_off : 0;
+  if (ntiles_global) *ntiles_global = h->part ? h->part_ntiles_global : h->total_tiles;
+  return h->part ? LEV_OK : fail(LEV_ERR_STATE, "not a partition engine");
+}
+
+int lev_part_step_begin(LevEngine *h, float dt, void *partials_dev) {
+  int rc = part_check(h);
+  if (rc != LEV_OK) return rc;
+  if (!std::isfinite(dt)) return fail(LEV_ERR_ARG, "dt is not finite");
+  if (!partials_dev) return fail(LEV_ERR_ARG, "partials buffer is null");
+  DeviceScope ds(h->device);
+  StepArgs a = make_args(h, dt, nullptr, 0, nullptr);
+  a.partials = static_cast<float2 *>(partials_dev);
+  a.hubs = nullptr;
+  return launch_step(h, a);
+}
+
+int lev_part_step_end(LevEngine *h, float dt, const void *partials_all_dev,
+                      float *r_dev) {
+  int rc = part_check(h);
+  if (rc != LEV_OK) return rc;
+  if (!std::isfinite(dt)) return fail(LEV_ERR_ARG, "dt is not finite");
+  if (!partials_all_dev) return fail(LEV_ERR_ARG, "partials buffer is null");
+  DeviceScope ds(h->device);
+  part_finish_kernel<<<1, 32, 0, h->stream>>>(
+      h->d_nets, h->d_st, static_cast<const float2 *>(partials_all_dev),
+      h->part_ntiles_global, h->part_N_global, dt, r_dev, h->d_rmap);
+  LEV_TRY_CUDA(cudaGetLastError());
+  return LEV_OK;
+}
+
+int lev_part_pack(LevEngine *h, const int32_t *idx_dev, int32_t n, float *out_dev) {
+  int rc = part_check(h);
+  if (rc != LEV_OK) return rc;
+  if (n < 0) return fail(LEV_ERR_ARG, "n must be >= 0");
+  if (n == 0) return LEV_OK;
+  if (!idx_dev || !out_dev) return fail(LEV_ERR_ARG, "null device pointer");
+  DeviceScope ds(h->device);
+  const int blocks = std::min((n + 255) / 256, 148 * 8);
+  part_pack_kernel<<<blocks, 256, 0, h->stream>>>(h->d_theta, h->h_nets[0].N, idx_dev, n,
+                                                  out_dev);
+  LEV_TRY_CUDA(cudaGetLastError());
+  return LEV_OK;
+}
+
+int lev_part_unpack(LevEngine *h, const int32_t *idx_dev, int32_t n, const float *in_dev) {
+  int rc = part_check(h);
+  if (rc != LEV_OK) return rc;
+  if (n < 0) return fail(LEV_ERR_ARG, "n must be >= 0");
+  if (n == 0) return LEV_OK;
+  if (!idx_dev || !in_dev) return fail(LEV_ERR_ARG, "null device pointer");
+  DeviceScope ds(h->device);
+  const NetDesc &nd = h->h_nets[0];
+  const int blocks = std::min((n + 255) / 256, 148 * 8);
+  part_unpack_kernel<<<blocks, 256, 0, h->stream>>>(h->d_st, h->d_ring + nd.ring_off, nd.N,
+                                                    nd.Np, h->part_halo, idx_dev, n, in_dev);
+  LEV_TRY_CUDA(cudaGetLastError());
+  return LEV_OK;
+}
+
+int lev_part_fill_halo(LevEngine *h, const float *theta_halo) {
+  int rc = part_check(h);
+  if (rc != LEV_OK) return rc;
+  if (h->part_halo == 0) return LEV_OK;
+  if (!theta_halo) return fail(LEV_ERR_ARG, "theta_halo is null");
+  DeviceScope ds(h->device);
+  return fill_ext_columns(h, h->part_halo, theta_halo);
 }
 
 }  // extern "C"
@@ -3784,9 +4011,10 @@ __global__ void __launch_bounds__(kTile) noalloc_step_kernel(const NoAllocArgs a
 }
 
 // Device address of g_noalloc_scratch per device, looked up on the first
-// call made with that device current.
+// call made with that device current.  Atomic: two threads making their first
+// call on one device at once both store the same address.
 constexpr int kNoAllocMaxDevices = 64;
-static unsigned int *g_noalloc_addr[kNoAllocMaxDevices] = {};
+static std::atomic<unsigned int *> g_noalloc_addr[kNoAllocMaxDevices] = {};
 
 }  // namespace lev
 
@@ -3806,8 +4034,8 @@ extern "C" int lev_step_noalloc(int32_t N, int32_t max_delay, int64_t t,
   if (max_delay < 0 || max_delay > 255)
     return fail(LEV_ERR_ARG, "lev_step_noalloc: max_delay must be in [0,255]");
   if (t < 0) return fail(LEV_ERR_ARG, "lev_step_noalloc: t must be >= 0");
-  if (!row_ptr || !theta || !theta_hat || !omega || !omega_hat || !ring ||
-      !gain || !r_out)
+  if (!row_ptr || !col_idx || !delays || !weights || !theta || !theta_hat ||
+      !omega || !omega_hat || !ring || !gain || !r_out)
     return fail(LEV_ERR_ARG, "lev_step_noalloc: null device pointer");
   if (!std::isfinite(dt)) return fail(LEV_ERR_ARG, "lev_step_noalloc: dt is not finite");
   if (math_mode != LEV_MATH_REFERENCE && math_mode != LEV_MATH_ACCURATE)
@@ -3821,12 +4049,13 @@ extern "C" int lev_step_noalloc(int32_t N, int32_t max_delay, int64_t t,
   LEV_TRY_CUDA(cudaGetDevice(&dev));
   if (dev < 0 || dev >= kNoAllocMaxDevices)
     return fail(LEV_ERR_ARG, "lev_step_noalloc: device ordinal too large");
-  if (!g_noalloc_addr[dev]) {
+  unsigned int *scratch = g_noalloc_addr[dev].load(std::memory_order_acquire);
+  if (!scratch) {
     void *addr = nullptr;
     LEV_TRY_CUDA(cudaGetSymbolAddress(&addr, g_noalloc_scratch));
-    g_noalloc_addr[dev] = static_cast<unsigned int *>(addr);
+    scratch = static_cast<unsigned int *>(addr);
+    g_noalloc_addr[dev].store(scratch, std::memory_order_release);
   }
-  unsigned int *scratch = g_noalloc_addr[dev];
   cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
 
   NoAllocArgs a;

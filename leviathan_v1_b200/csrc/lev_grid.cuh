@@ -29,7 +29,7 @@
 // Arithmetic and summation order are those of step_kernel: results are
 // bitwise the same as stepping with step_kernel.
 //
-// The barrier's wait is bounded (kGridWaitNs of globaltimer): on a timeout
+// The barrier's wait is bounded (GridWait, 2 s by default): on a timeout
 // the CTA writes 1 to the error flag (mapped host memory), leaves the step
 // loop and writes nothing back; the host reports the error.
 
@@ -40,7 +40,17 @@
 namespace lev {
 
 constexpr int kGridLPR = 4;                               // lanes per row
-constexpr unsigned long long kGridWaitNs = 2000000000ull;  // barrier wait limit
+constexpr unsigned long long kGridWaitNs = 2000000000ull;  // default wait limit
+
+// Bound of every grid-barrier wait of a launch.  `extra` is 0 in normal use;
+// a positive value makes each wait expect that many arrivals more than the
+// grid makes, so the first wait runs out after `ns` -- the timeout path can
+// then be exercised by a test without faulting or hanging the GPU.
+struct GridWait {
+  unsigned long long ns;  // limit of one wait, globaltimer nanoseconds
+  unsigned extra;
+  unsigned pad;
+};
 
 struct GridArgs {
   const NetDesc *net;
@@ -59,6 +69,7 @@ struct GridArgs {
   unsigned *bar;     // arrival counter, zero at launch
   int early;         // no delay is 0: wait for barrier t after step t+1's edges
   int *err;          // error flag (mapped host memory)
+  GridWait wait;     // bound of the barrier waits
   float *r_hist;     // [n] (row rpos + k), or null
   int r_cap;
   int n_steps;
@@ -99,13 +110,14 @@ __device__ __forceinline__ void grid_arrive(unsigned *bar) {
 }
 
 // Wait: every thread of the CTA calls it; thread 0 waits (acquire) until
-// `target` arrivals, at most kGridWaitNs.  Returns false after a timeout, in
-// every thread.
-__device__ __forceinline__ bool grid_wait(unsigned *bar, unsigned target, int *err, int *s_ok) {
+// `target` arrivals (plus gw.extra), at most gw.ns.  Returns false after a
+// timeout, in every thread.
+__device__ __forceinline__ bool grid_wait(unsigned *bar, unsigned target, int *err, int *s_ok,
+                                          const GridWait &gw) {
   if (threadIdx.x == 0) {
     const unsigned long long t0 = global_ns();
-    while (ld_acquire_gpu(bar) < target) {
-      if (global_ns() - t0 > kGridWaitNs) {
+    while (ld_acquire_gpu(bar) < target + gw.extra) {
+      if (global_ns() - t0 > gw.ns) {
         *reinterpret_cast<volatile int *>(err) = 1;
         *s_ok = 0;
         break;
@@ -218,7 +230,7 @@ __global__ void __launch_bounds__(kGridLPR * R, 256 / R) grid_kernel(const GridA
     // with zero delays: barrier step-1 before the gathers; the warp sums are
     // in flight during the predictor and the edge work
     if (step > 0 && !a.early) {
-      if (!(ok = grid_wait(a.bar, (unsigned)step * G, a.err, &s_ok))) break;
+      if (!(ok = grid_wait(a.bar, (unsigned)step * G, a.err, &s_ok, a.wait))) break;
       stage_sums(step - 1);
     }
     // ---- predictor (row's first lane) --------------------------------------
@@ -288,7 +300,7 @@ __global__ void __launch_bounds__(kGridLPR * R, 256 / R) grid_kernel(const GridA
     // ---- r and gain of the previous step (warp 0, from the staged sums) ----
     if (step > 0) {
       if (a.early) {
-        if (!(ok = grid_wait(a.bar, (unsigned)step * G, a.err, &s_ok))) break;
+        if (!(ok = grid_wait(a.bar, (unsigned)step * G, a.err, &s_ok, a.wait))) break;
         stage_sums(step - 1);
       }
       if (warp == 0) {
@@ -342,7 +354,7 @@ __global__ void __launch_bounds__(kGridLPR * R, 256 / R) grid_kernel(const GridA
     grid_arrive(a.bar);
   }
   // CTA 0 needs every warp sum of the last step
-  if (ok && a.n_steps > 0 && cta == 0) ok = grid_wait(a.bar, (unsigned)a.n_steps * G, a.err, &s_ok);
+  if (ok && a.n_steps > 0 && cta == 0) ok = grid_wait(a.bar, (unsigned)a.n_steps * G, a.err, &s_ok, a.wait);
   if (!ok) return;  // barrier timeout: the host reports it
   // ---- r of the last step (CTA 0), then write the state back ---------------
   if (a.n_steps > 0 && cta == 0 && warp == 0) {

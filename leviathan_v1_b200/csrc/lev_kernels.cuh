@@ -69,7 +69,9 @@ struct NetDesc {
   int ntiles;     // 256-row tiles of this network
   int part_off;   // first partial-sum slot
   int tile_off;   // first tile (CTA) of this network in the grid
-  int pad0;
+  int dist;       // 1: partition of a network split over GPUs (lev_part.cuh):
+                  // step_kernel stops after the tile partials, which go to
+                  // their global tile positions (part_off = first global tile)
   float eta, lam, gamma, alpha, kappa_w, w_min, w_max, r0;
   float beta, mu, g_rest, g_min, g_max;
   int ctrl;
@@ -402,9 +404,13 @@ __global__ void __launch_bounds__(kTile, MINB) step_kernel(const StepArgs a) {
     }
     if (lane == 0) {
       a.partials[nd.part_off + row0 / kTile] = make_float2(my_cos, my_sin);
-      __threadfence();
-      const unsigned prev = atomicAdd(&ns->ticket, 1u);
-      s_last = (prev == (unsigned)(nd.ntiles - 1));
+      if (nd.dist) {
+        s_last = 0;  // r of the whole network: part_finish_kernel
+      } else {
+        __threadfence();
+        const unsigned prev = atomicAdd(&ns->ticket, 1u);
+        s_last = (prev == (unsigned)(nd.ntiles - 1));
+      }
     }
   }
   __syncthreads();
@@ -470,11 +476,12 @@ __global__ void ring_fill_kernel(const float *__restrict__ theta,
 // CSR -> SELL-32 for one network: entry k of row i goes to
 // sl_off[slice_base + i/32] + 32k + i%32.  One thread per row.
 // mode 0: pack (col, delay) into sl_cd and copy weights, validating
-//         col in [0,N) and delay <= max_delay (bits 1, 2 of *err); bit 4
-//         reports a zero delay;
+//         col in [0,ncols) and delay <= max_delay (bits 1, 2 of *err); bit 4
+//         reports a zero delay (ncols = N, or N plus the halo columns of a
+//         partition, lev_part.cuh);
 // mode 1: weights only, CSR -> SELL;   mode 2: weights only, SELL -> CSR.
 __global__ void sell_convert_kernel(int mode, const int *__restrict__ row_ptr,
-                                    int N, long long slice_base,
+                                    int N, int ncols, long long slice_base,
                                     const long long *__restrict__ sl_off,
                                     const int *__restrict__ col,
                                     const uint8_t *__restrict__ delays,
@@ -492,7 +499,7 @@ __global__ void sell_convert_kernel(int mode, const int *__restrict__ row_ptr,
       if (mode == 0) {
         const int c = col[e];
         const int d = delays[e];
-        if (c < 0 || c >= N) bad |= 1u;
+        if (c < 0 || c >= ncols) bad |= 1u;
         if (d > max_delay) bad |= 2u;
         if (d == 0) bad |= 4u;  // not an error: rules out two steps per launch
         sl_cd[idx] = ((uint32_t)c << 8) | (uint32_t)d;

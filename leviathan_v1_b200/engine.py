@@ -306,6 +306,12 @@ class _EngineBase:
         rows_per_cta 64, 128 or 256 picks the CTA size (0 keeps it)."""
         check(self._lib.lev_set_grid_mode(self.handle, 1 if enabled else 0, int(rows_per_cta)))
 
+    def set_grid_wait(self, limit_ns: int = 2_000_000_000, extra_arrivals: int = 0) -> None:
+        """Bound of the grid-barrier waits (default 2 s).  ``extra_arrivals``
+        > 0 makes the next grid-resident block's first wait run out: for
+        tests of the timeout path (see ``lev_set_grid_wait``)."""
+        check(self._lib.lev_set_grid_wait(self.handle, int(limit_ns), int(extra_arrivals)))
+
     # -- two steps per launch (step blocks; no zero delays) -----------------
     def pair_info(self) -> list:
         """Per degree class: whether two steps per launch are possible

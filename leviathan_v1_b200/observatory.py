@@ -8,9 +8,9 @@ Same constructor, methods and return values.  Differences, all deliberate:
   python/leviathan_h100.py:31-34, so its topology changes from run to run);
 * a prebuilt :class:`~leviathan_v1_b200.graphs.Network` can be passed instead
   of (N, k, max_delay, seed) to run a benchmark configuration;
-* ``run_baseline`` advances the engine in step blocks of ``log_interval``
-  steps (one CUDA-graph replay per block) instead of one host round trip per
-  step; it records the same r(t) for every step and prints at the same
+* ``run_baseline`` and ``run_with_stimulus`` advance the engine in step
+  blocks (one CUDA-graph replay per block) instead of one host round trip per
+  step; they record the same r(t) for every step and print at the same
   intervals.
 """
 
@@ -119,23 +119,24 @@ class LeviathanObservatory:
         self.engine.reset_weights(weights)
 
     def get_vram_report(self):
-        """Formatted device-memory report (python/leviathan_h100.py:112-138);
-        the breakdown is of this engine's layout."""
-        bs = self.max_delay + 2
-        Np = (self.N + 31) // 32 * 32
-        breakdown = {
-            "History Buffer": bs * Np * 4,
-            "Topology (CSR)": (self.N + 1) * 4 + self.nnz * (4 + 4),
-            "Node States": self.N * 4 * 4,
-            "Reduction Buffers": ((self.N + 255) // 256) * 8,
-        }
-        report = f"VRAM Usage Report (N={self.N}, E={self.nnz})\n"
-        report += f"{'-' * 40}\n"
-        for k, v in breakdown.items():
-            report += f"{k:20s} : {v / (1024 * 1024):8.2f} MB\n"
-        report += f"{'-' * 40}\n"
-        report += f"{'TOTAL (Measured)':20s} : {self.get_vram_usage() / (1024 * 1024):8.2f} MB\n"
-        return report
+        """Device-memory report with the layout of python/leviathan_h100.py:
+        112-138 (a title line, one line per part, the measured total).  The
+        parts are this engine's own buffers: the slot-major delay ring of
+        max_delay+2 slots over N rounded up to 32, the four node arrays, the
+        per-tile partial sums, and the SELL-32 edge streams with everything
+        else as the remainder of the measured total."""
+        total = self.get_vram_usage()
+        ring = (self.max_delay + 2) * (-(-self.N // 32) * 32) * 4
+        nodes = 4 * 4 * self.N
+        partials = 8 * -(-self.N // 256)
+        parts = [("Delay ring", ring), ("Node state", nodes),
+                 ("Tile partials", partials),
+                 ("Edges + rest", max(total - ring - nodes - partials, 0))]
+        mib = float(1 << 20)
+        rule = "-" * 40
+        body = "".join(f"{name:20s} : {nbytes / mib:8.2f} MB\n" for name, nbytes in parts)
+        return (f"VRAM Usage Report (N={self.N}, E={self.nnz})\n{rule}\n{body}{rule}\n"
+                f"{'TOTAL (Measured)':20s} : {total / mib:8.2f} MB\n")
 
     # -- runs (python/leviathan_h100.py:140-196) -----------------------------
     def run_baseline(self, num_steps=500, log_interval=100):
@@ -157,25 +158,42 @@ class LeviathanObservatory:
 
     def run_with_stimulus(self, num_steps=200, stimulus_start=100,
                           stimulus_nodes=None, stimulus_strength=2.0):
-        """External phase kick at ``stimulus_start`` (TMS-style)."""
-        if stimulus_nodes is None:
-            stimulus_nodes = list(range(10))
+        """External phase kick (TMS-style), python/leviathan_h100.py:157-196.
+
+        Same trajectory as the reference's loop: steps 0 .. stimulus_start
+        run, then ``stimulus_strength`` is added to the phase of every listed
+        node (a node listed twice is kicked twice), all phases are taken modulo
+        2 pi in float32 and uploaded with ``set_phase_snapshot`` (which refills
+        the delay ring), and the remaining steps run.  Steps advance in blocks
+        (one engine call each) that end at the kick and at every 50th step,
+        where the progress line is printed.  Returns r of the last
+        ``num_steps`` steps.
+        """
+        nodes = np.arange(10) if stimulus_nodes is None else np.asarray(stimulus_nodes)
         self._log(f"[Observatory] Stimulus run: {num_steps} steps, start={stimulus_start}")
-        start = time.time()
-        for i in range(num_steps):
-            r = self.step()
-            if i == stimulus_start:
-                theta = self.get_phase_snapshot()
-                for node in stimulus_nodes:
-                    theta[node] += stimulus_strength
-                theta = theta % (2 * np.pi)
-                self.set_phase_snapshot(theta)
-                self._log(f"  [STIMULUS] Applied phase kick to {len(stimulus_nodes)} nodes")
-            if (i + 1) % 50 == 0:
-                phase = "ACTIVE" if i >= stimulus_start else "baseline"
-                fps = (i + 1) / max(time.time() - start, 1e-12)
-                self._log(f"  Step {i + 1:3d} [{phase}]: r={r:.4f} ({fps:.1f} FPS)")
-        self._log(f"[Observatory] Complete in {time.time() - start:.2f}s\n")
+        self._log(f"[Observatory] Target nodes: {list(nodes[:5])}... (total {nodes.size})")
+        self._log(f"[Observatory] Strength: {stimulus_strength}\n")
+        kick_after = stimulus_start + 1  # the kick follows step index stimulus_start
+        report_every = 50
+        t0 = time.time()
+        done = 0
+        while done < num_steps:
+            stops = [num_steps, (done // report_every + 1) * report_every]
+            if done < kick_after:
+                stops.append(kick_after)
+            end = min(stops)
+            rs = self.step_n(end - done)
+            done = end
+            if done == kick_after:
+                phases = self.get_phase_snapshot()
+                np.add.at(phases, nodes, np.float32(stimulus_strength))
+                self.set_phase_snapshot(np.remainder(phases, 2 * np.pi))
+                self._log(f"  [STIMULUS] Applied phase kick to {nodes.size} nodes")
+            if done % report_every == 0:
+                label = "ACTIVE" if done > stimulus_start else "baseline"
+                rate = done / max(time.time() - t0, 1e-12)
+                self._log(f"  Step {done:3d} [{label}]: r={rs[-1]:.4f} ({rate:.1f} FPS)")
+        self._log(f"[Observatory] Complete in {time.time() - t0:.2f}s\n")
         return self.r_history[-num_steps:]
 
     # -- snapshots (python/leviathan_h100.py:198-219) ------------------------

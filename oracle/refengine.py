@@ -20,7 +20,9 @@ LIBS = {
     "sm100a": os.path.join(REF_DIR, "libleviathan_ref.so"),
     "stock": os.path.join(REF_DIR, "libleviathan_ref_stock.so"),
 }
-REFERENCE_SRC = "/root/reference/src/cuda/leviathan_kernel.cu"
+# Where the reference sources lie (same variable as oracle/Makefile's REF).
+REFERENCE_ROOT = os.environ.get("LEVIATHAN_REF", "/root/reference")
+REFERENCE_SRC = os.path.join(REFERENCE_ROOT, "src", "cuda", "leviathan_kernel.cu")
 
 _P = C.c_void_p
 _cache: dict = {}
@@ -31,7 +33,8 @@ def build_if_possible() -> bool:
     machine only; the GPU machine uses the prebuilt files)."""
     if not os.path.exists(REFERENCE_SRC):
         return all(os.path.exists(p) for p in LIBS.values())
-    proc = subprocess.run(["make", "-s", "-C", HERE], capture_output=True, text=True)
+    proc = subprocess.run(["make", "-s", "-C", HERE, f"REF={REFERENCE_ROOT}"],
+                          capture_output=True, text=True)
     if proc.returncode != 0:
         raise RuntimeError("reference build failed:\n" + proc.stdout + proc.stderr)
     return True

@@ -1,13 +1,14 @@
-"""Representative workloads of each kernel, for profilers.
+"""Representative workloads of each kernel, for profilers (measurement
+tooling beside bench.py; not part of the package).
 
-    python -m leviathan_v1_b200.profile_cases step      [--N 1000000 --k 32 --steps 5]
-    python -m leviathan_v1_b200.profile_cases cluster   [--N 1000 --k 20 --steps 200]
-    python -m leviathan_v1_b200.profile_cases grid      [--N 10000 --k 20 --steps 200]
-    python -m leviathan_v1_b200.profile_cases batched   [--batch 128 --steps 20 --pair -1]
-    python -m leviathan_v1_b200.profile_cases adjoint   [--N 200000 --k 32 --T 100]
-    python -m leviathan_v1_b200.profile_cases adjgrid   [--N 10000 --k 20 --T 200]
-    python -m leviathan_v1_b200.profile_cases reservoir [--N 20000 --batch 8 --T 60]
-    python -m leviathan_v1_b200.profile_cases e2e       [--N 1000000 --k 32 --steps 500]
+    python profile_cases.py step      [--N 1000000 --k 32 --steps 5]
+    python profile_cases.py cluster   [--N 1000 --k 20 --steps 200]
+    python profile_cases.py grid      [--N 10000 --k 20 --steps 200]
+    python profile_cases.py batched   [--batch 128 --steps 20 --pair -1]
+    python profile_cases.py adjoint   [--N 200000 --k 32 --T 100]
+    python profile_cases.py adjgrid   [--N 10000 --k 20 --T 200]
+    python profile_cases.py reservoir [--N 20000 --batch 8 --T 60]
+    python profile_cases.py e2e       [--N 1000000 --k 32 --steps 500]
 
 Each runs a short, fixed amount of work on the current CUDA device (graphs
 built on the device, seeded) and prints one JSON line of timings; sizes are
@@ -19,9 +20,13 @@ from __future__ import annotations
 
 import argparse
 import json
+import os
+import sys
 import time
 
 import numpy as np
+
+sys.path.insert(0, os.path.dirname(os.path.abspath(__file__)))
 
 
 def _sync():
@@ -31,8 +36,8 @@ def _sync():
 
 
 def case_step(a):
-    from .engine import LeviathanEngine
-    from .graphs import make_network_gpu
+    from leviathan_v1_b200.engine import LeviathanEngine
+    from leviathan_v1_b200.graphs import make_network_gpu
 
     net = make_network_gpu(a.N, a.k, 0.1, a.max_delay, a.seed)
     e = LeviathanEngine(*net.engine_args())
@@ -46,8 +51,8 @@ def case_step(a):
 
 
 def case_cluster(a):
-    from .engine import LeviathanEngine
-    from .graphs import make_network_gpu
+    from leviathan_v1_b200.engine import LeviathanEngine
+    from leviathan_v1_b200.graphs import make_network_gpu
 
     net = make_network_gpu(a.N, a.k, 0.1, a.max_delay, a.seed)
     e = LeviathanEngine(*net.engine_args())
@@ -63,8 +68,8 @@ def case_cluster(a):
 
 
 def case_grid(a):
-    from .engine import LeviathanEngine
-    from .graphs import make_network_gpu
+    from leviathan_v1_b200.engine import LeviathanEngine
+    from leviathan_v1_b200.graphs import make_network_gpu
 
     net = make_network_gpu(a.N, a.k, 0.1, a.max_delay, a.seed)
     e = LeviathanEngine(*net.engine_args())
@@ -86,8 +91,8 @@ def case_batched(a):
     controller off), autotuned, then `steps` steps in step blocks.  `pair` >= 0
     sets that two-steps-per-launch variant for every class after the
     autotuner (under a profiler the autotuner's timings do not hold)."""
-    from .engine import BatchEngine
-    from .graphs import batch_specs, build_batch
+    from leviathan_v1_b200.engine import BatchEngine
+    from leviathan_v1_b200.graphs import batch_specs, build_batch
 
     specs = batch_specs(512, seed=0)[:a.batch]
     nets, params = build_batch(specs)
@@ -110,9 +115,9 @@ def case_batched(a):
 def case_adjoint(a):
     import torch
 
-    from .adjoint import Adjoint, simulate
-    from .engine import LeviathanEngine
-    from .graphs import make_network_gpu
+    from leviathan_v1_b200.adjoint import Adjoint, simulate
+    from leviathan_v1_b200.engine import LeviathanEngine
+    from leviathan_v1_b200.graphs import make_network_gpu
 
     net = make_network_gpu(a.N, a.k, 0.1, a.max_delay, a.seed)
     eng = LeviathanEngine(*net.engine_args(), math_mode="accurate")
@@ -136,8 +141,8 @@ def case_adjoint(a):
 def case_reservoir(a):
     import torch
 
-    from .graphs import make_network_gpu
-    from .reservoir import DifferentiableReservoir, make_inputs
+    from leviathan_v1_b200.graphs import make_network_gpu
+    from leviathan_v1_b200.reservoir import DifferentiableReservoir, make_inputs
 
     net = make_network_gpu(a.N, a.k, 0.1, a.max_delay, a.seed)
     m = DifferentiableReservoir(net, a.batch, n_input=min(256, a.N // 4), T=a.T,
@@ -158,8 +163,8 @@ def case_reservoir(a):
 def case_e2e(a):
     """Breakdown of the whole job through the public API: engine
     construction from host arrays, K synchronous steps, snapshot."""
-    from .engine import LeviathanEngine
-    from .graphs import make_network_gpu
+    from leviathan_v1_b200.engine import LeviathanEngine
+    from leviathan_v1_b200.graphs import make_network_gpu
 
     net = make_network_gpu(a.N, a.k, 0.1, a.max_delay, a.seed)
     e = LeviathanEngine(*net.engine_args())  # warm-up: context, module load

@@ -75,10 +75,24 @@ def test_observatory_runs_like_the_reference_host_api():
     ra = a.run_baseline(num_steps=300, log_interval=100).copy()
     rb = np.array([b.step() for _ in range(300)], np.float32)
     np.testing.assert_array_equal(ra, rb)  # step blocks == single steps
-    rs = a.run_with_stimulus(num_steps=60, stimulus_start=20)
-    assert rs.shape == (60,) and a.step_count == 360
+    nodes = [3, 7, 7, 1999]  # a repeated node is kicked twice
+    rs = a.run_with_stimulus(num_steps=120, stimulus_start=64, stimulus_nodes=nodes,
+                             stimulus_strength=2.5)
+    # the reference's loop (python/leviathan_h100.py:178-189): one step per
+    # call, the kick after step index stimulus_start
+    ref = []
+    for i in range(120):
+        ref.append(b.step())
+        if i == 64:
+            th = b.get_phase_snapshot()
+            for n in nodes:
+                th[n] += 2.5
+            b.set_phase_snapshot(th % (2 * np.pi))
+    np.testing.assert_array_equal(rs, np.array(ref, np.float32))
+    np.testing.assert_array_equal(a.get_phase_snapshot(), b.get_phase_snapshot())
+    assert rs.shape == (120,) and a.step_count == 420
     st = a.statistics()
-    assert st["steps"] == 360 and 0 <= st["min_r"] <= st["max_r"] <= 1
+    assert st["steps"] == 420 and 0 <= st["min_r"] <= st["max_r"] <= 1
     th = a.get_phase_snapshot()
     assert th.shape == (2000,) and np.all((th >= 0) & (th < 2 * np.pi + 1e-5))
     a.set_phase_snapshot(np.zeros(2000))
