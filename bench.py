@@ -625,7 +625,9 @@ def run_ours(args, rank, world, local):
     torch.cuda.synchronize()
     e2e_s = time.perf_counter() - t0
     e2e_parts = {"construct_s": t1 - t0, "step_n_s": t2 - t1,
-                 "get_theta_s": e2e_s - (t2 - t0)}
+                 "get_theta_s": e2e_s - (t2 - t0),
+                 "construct_ms_by_phase": e2.create_profile(),
+                 "h2d_GBps_of_construct": h2d_bytes(N, E) / (t1 - t0) / 1e9}
     e2.close()
     e2e_s = max_over_ranks(e2e_s, world)
     # the same job with one step(dt) call per step (reference call pattern)

@@ -121,6 +121,13 @@ int lev_batch_create(LevEngine **out, int32_t num_nets, const int32_t *N,
 /* Replaces leviathan_free (leviathan_kernel.cu:455-478). */
 int lev_destroy(LevEngine *h);
 
+/* Wall-clock milliseconds of the phases of the engine's creation (no
+ * reference counterpart; for tuning construction): ms_out[6] = host-side
+ * validation and layout, device resources (stream, allocations), node-array
+ * uploads, edge-array uploads (host side), CSR -> SELL conversion (waits for
+ * the uploads), ring fill and the final synchronisation. */
+int lev_create_profile(const LevEngine *h, double *ms_out);
+
 /* Shape queries. */
 int lev_num_nets(const LevEngine *h, int32_t *out);
 int lev_total_nodes(const LevEngine *h, int64_t *out);
@@ -258,7 +265,8 @@ int lev_set_cluster_mode(LevEngine *h, int32_t enabled);
  * The barrier wait is bounded; a timeout makes lev_step_n / lev_sync return
  * LEV_ERR_CUDA and disables the path.  Results are bitwise those of the
  * per-step kernel.  The cluster path takes precedence when both are enabled.
- * lev_grid_info: rows_per_cta in use; eligible_rows_mask = OR of the
+ * lev_grid_info: enabled = eligible and allowed (the path step blocks use;
+ * 0 after a timeout); rows_per_cta in use; eligible_rows_mask = OR of the
  * eligible rows-per-CTA values.  lev_set_grid_mode: enabled 0 forces the
  * per-step kernel; rows_per_cta 0 keeps the current choice. */
 int lev_grid_info(const LevEngine *h, int32_t *eligible, int32_t *enabled, int32_t *ctas,

@@ -9,6 +9,7 @@
 
 #include <algorithm>
 #include <atomic>
+#include <chrono>
 #include <cmath>
 #include <cstdio>
 #include <cstring>
@@ -224,6 +225,9 @@ struct LevEngine {
   unsigned *d_gbar = nullptr;
   int *h_gerr = nullptr, *d_gerr = nullptr;  // barrier timeout flag (mapped)
   GridWait grid_wait = {kGridWaitNs, 0u, 0u};  // bound of the barrier waits
+
+  // wall-clock ms of the phases of creation (lev_create_profile)
+  double create_ms[6] = {0, 0, 0, 0, 0, 0};
 
   // partition of a network split over GPUs (lev_part.cuh, lev_part_*): own
   // rows stepped here, halo phases in ring columns N .. N + part_halo - 1
@@ -1007,6 +1011,11 @@ int fill_ext_columns(LevEngine *h, int n_ext, const float *theta_ext) {
   return LEV_OK;
 }
 
+double ms_since(std::chrono::steady_clock::time_point t0) {
+  return std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0)
+      .count();
+}
+
 int create_impl(LevEngine **out, int num_nets, const int32_t *Ns,
                 const int32_t *mds, const int32_t *rp_cat,
                 const int32_t *col_cat, const uint8_t *d_cat,
@@ -1027,7 +1036,14 @@ int create_impl(LevEngine **out, int num_nets, const int32_t *Ns,
   if (math_mode != LEV_MATH_REFERENCE && math_mode != LEV_MATH_ACCURATE)
     return fail(LEV_ERR_ARG, "math_mode must be 0 (reference) or 1");
 
+  const auto t_start = std::chrono::steady_clock::now();
+  double t_mark = 0.0;
   LevEngine *h = new LevEngine();
+  auto mark = [&](int k) {
+    const double t = ms_since(t_start);
+    h->create_ms[k] = t - t_mark;
+    t_mark = t;
+  };
   h->num_nets = num_nets;
   h->math_mode = math_mode;
   h->h_nets.resize(num_nets);
@@ -1175,6 +1191,7 @@ int create_impl(LevEngine **out, int num_nets, const int32_t *Ns,
     }
   }
 
+  mark(0);
   // ---- device resources ----------------------------------------------------
   cudaError_t ce = cudaGetDevice(&h->device);
   if (ce != cudaSuccess) {
@@ -1238,6 +1255,7 @@ int create_impl(LevEngine **out, int num_nets, const int32_t *Ns,
                                   cudaGetErrorString(ce));
   }
 
+  mark(1);
   // ---- uploads -------------------------------------------------------------
   unsigned *d_err = nullptr;
   uint8_t *d_tmp = nullptr;    // delays, CSR order
@@ -1286,6 +1304,7 @@ int create_impl(LevEngine **out, int num_nets, const int32_t *Ns,
                       h->stream) != cudaSuccess)
     return cleanup_fail(LEV_ERR_CUDA, "memset failed");
 
+  mark(2);
   if (edge_off > 0) {
     if (cudaMalloc(&d_tmp, edge_off) != cudaSuccess ||
         cudaMalloc(&d_tcol, sizeof(int) * edge_off) != cudaSuccess ||
@@ -1297,6 +1316,7 @@ int create_impl(LevEngine **out, int num_nets, const int32_t *Ns,
     LEV_UP(d_tmp, d_cat, edge_off);
     if (cudaMemsetAsync(d_err, 0, sizeof(unsigned), h->stream) != cudaSuccess)
       return cleanup_fail(LEV_ERR_CUDA, "memset failed");
+    mark(3);
     for (int n = 0; n < num_nets; ++n) {
       const NetDesc &d = h->h_nets[n];
       if (h->net_E[n] == 0) continue;
@@ -1322,6 +1342,7 @@ int create_impl(LevEngine **out, int num_nets, const int32_t *Ns,
     if (herr & 2u)
       return cleanup_fail(LEV_ERR_ARG, "delay larger than max_delay");
     h->pair_ok = !(herr & 4u);
+    mark(4);
     cudaFree(d_tmp);
     cudaFree(d_tcol);
     cudaFree(d_tw);
@@ -1363,6 +1384,7 @@ int create_impl(LevEngine **out, int num_nets, const int32_t *Ns,
     return fail(LEV_ERR_CUDA,
                 std::string("engine init failed: ") + cudaGetErrorString(ce));
   }
+  mark(5);
   *out = h;
   return LEV_OK;
 }
@@ -1926,7 +1948,7 @@ int lev_grid_info(const LevEngine *h, int32_t *eligible, int32_t *enabled, int32
   const int R = h->grid_R;
   const int ri = grid_r_index(R);
   if (eligible) *eligible = h->grid_ok ? 1 : 0;
-  if (enabled) *enabled = h->use_grid ? 1 : 0;
+  if (enabled) *enabled = (h->grid_ok && h->use_grid) ? 1 : 0;  // in use by step blocks
   if (ctas) *ctas = (h->grid_ok && R > 0) ? (h->h_nets[0].N + R - 1) / R : 0;
   if (rows_per_cta) *rows_per_cta = h->grid_ok ? R : 0;
   if (smem_bytes) *smem_bytes = h->grid_ok ? (int64_t)h->grid_smem_R[ri] : 0;
@@ -1965,6 +1987,12 @@ int lev_set_grid_wait(LevEngine *h, uint64_t limit_ns, uint32_t extra_arrivals) 
   if (rc != LEV_OK) return rc;
   h->grid_wait.ns = limit_ns;
   h->grid_wait.extra = extra_arrivals;
+  return LEV_OK;
+}
+
+int lev_create_profile(const LevEngine *h, double *ms_out) {
+  if (!h || !ms_out) return fail(LEV_ERR_ARG, "null argument");
+  for (int k = 0; k < 6; ++k) ms_out[k] = h->create_ms[k];
   return LEV_OK;
 }
 

@@ -306,6 +306,13 @@ class _EngineBase:
         rows_per_cta 64, 128 or 256 picks the CTA size (0 keeps it)."""
         check(self._lib.lev_set_grid_mode(self.handle, 1 if enabled else 0, int(rows_per_cta)))
 
+    def create_profile(self) -> dict:
+        """Milliseconds of the phases of this engine's creation."""
+        ms = (C.c_double * 6)()
+        check(self._lib.lev_create_profile(self.handle, ms))
+        keys = ("layout", "resources", "node_uploads", "edge_uploads", "convert", "fill")
+        return {k: float(v) for k, v in zip(keys, ms)}
+
     def set_grid_wait(self, limit_ns: int = 2_000_000_000, extra_arrivals: int = 0) -> None:
         """Bound of the grid-barrier waits (default 2 s).  ``extra_arrivals``
         > 0 makes the next grid-resident block's first wait run out: for

@@ -119,5 +119,7 @@ def test_adjoint_grid_wait_timeout_is_reported():
     assert "timed out" in str(err)
     assert not info["enabled"]  # the adjoint stopped using grid segments
     np.testing.assert_array_equal(r, r_ref)  # per-step launches, same trajectory
+    # the per-step reverse kernel scatters with atomics, so two runs agree to
+    # summation order only
     for a, b in zip(g, g_ref):
-        np.testing.assert_array_equal(a, b)
+        assert np.linalg.norm(a - b) <= 1e-5 * np.linalg.norm(b)
