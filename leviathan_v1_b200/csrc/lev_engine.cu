@@ -226,6 +226,10 @@ struct LevEngine {
   int *h_gerr = nullptr, *d_gerr = nullptr;  // barrier timeout flag (mapped)
   GridWait grid_wait = {kGridWaitNs, 0u, 0u};  // bound of the barrier waits
 
+  // one device allocation holding the arrays sized at creation
+  void *slab = nullptr;
+  size_t slab_bytes = 0;
+
   // wall-clock ms of the phases of creation (lev_create_profile)
   double create_ms[6] = {0, 0, 0, 0, 0, 0};
 
@@ -278,28 +282,37 @@ void free_engine(LevEngine *h) {
     if (kv.second.graph) cudaGraphDestroy(kv.second.graph);
   }
   h->graphs.clear();
-  cudaFree(h->d_nets);
-  cudaFree(h->d_st);
-  cudaFree(h->d_tiles);
-  cudaFree(h->d_row_ptr);
-  cudaFree(h->d_sl_off);
-  cudaFree(h->d_sl_len);
-  cudaFree(h->d_sl_cd);
-  cudaFree(h->d_sl_w);
-  cudaFree(h->d_theta);
-  cudaFree(h->d_theta_hat);
-  cudaFree(h->d_omega);
-  cudaFree(h->d_omega_hat);
-  cudaFree(h->d_ring);
-  cudaFree(h->d_part);
-  cudaFree(h->d_pend);
-  cudaFree(h->d_w_spec);
-  cudaFree(h->d_thh_spec);
-  cudaFree(h->d_omh_spec);
-  cudaFree(h->d_class_nets);
-  cudaFree(h->d_rhist);
-  cudaFree(h->d_gwsum);
-  cudaFree(h->d_gbar);
+  // arrays inside the creation slab go with it (a pointer swapped with a
+  // separately allocated buffer, as the speculative weights are, is freed
+  // on its own)
+  auto dfree = [h](void *p) {
+    const char *c = static_cast<const char *>(p);
+    const char *b = static_cast<const char *>(h->slab);
+    if (p && !(b && c >= b && c < b + h->slab_bytes)) cudaFree(p);
+  };
+  dfree(h->d_nets);
+  dfree(h->d_st);
+  dfree(h->d_tiles);
+  dfree(h->d_row_ptr);
+  dfree(h->d_sl_off);
+  dfree(h->d_sl_len);
+  dfree(h->d_sl_cd);
+  dfree(h->d_sl_w);
+  dfree(h->d_theta);
+  dfree(h->d_theta_hat);
+  dfree(h->d_omega);
+  dfree(h->d_omega_hat);
+  dfree(h->d_ring);
+  dfree(h->d_part);
+  dfree(h->d_pend);
+  dfree(h->d_w_spec);
+  dfree(h->d_thh_spec);
+  dfree(h->d_omh_spec);
+  dfree(h->d_class_nets);
+  dfree(h->d_rhist);
+  dfree(h->d_gwsum);
+  dfree(h->d_gbar);
+  if (h->slab) cudaFree(h->slab);
   if (h->h_gerr) cudaFreeHost(h->h_gerr);
   if (h->h_rmap) cudaFreeHost(h->h_rmap);
   if (h->h_rstage) cudaFreeHost(h->h_rstage);
@@ -900,78 +913,159 @@ int write_state(LevEngine *h, int n, const NetState &s) {
   return LEV_OK;
 }
 
-// Host-to-device upload of a caller's (usually pageable) array.  The driver
-// copies pageable memory through its own staging at one host thread's memcpy
-// speed; here the host side is split over several threads, each filling a
-// pinned staging buffer of its own and issuing the DMA of that chunk on the
-// engine's stream while it fills the next.  The staging buffers (kStageBufs x
-// kStageBytes of pinned memory) are allocated on the first large upload of
-// the process and kept for later ones.  Small or already pinned sources take
-// one cudaMemcpyAsync.  The source is fully read when this returns.
-constexpr size_t kStageBytes = 4u << 20;
-constexpr int kStageBufs = 8;
+// Host <-> device transfers of caller (pageable) memory through pinned
+// staging.  The driver moves pageable memory through its own staging at one
+// host thread's memcpy speed; here a transfer is cut into jobs of at most
+// kStageBytes, and up to kStageThreads host threads each fill a pinned
+// buffer of their own (a copy, or the SELL-32 packing of a range of slices)
+// and issue its DMA on the engine stream, with two buffers per thread so one
+// is filled while the other's DMA runs.  The buffers are allocated on the
+// first large transfer of the process (on that device) and kept.
+constexpr size_t kStageBytes = 2u << 20;
+constexpr int kStageThreads = 16;
+constexpr int kStageBufs = 2 * kStageThreads;
+constexpr int kStageDevices = 64;
 struct StagePool {
   std::mutex mu;
-  int device = -1;  // device of the events
   int nbuf = 0;
   void *buf[kStageBufs] = {};
   cudaEvent_t ev[kStageBufs] = {};
 };
-static StagePool g_stage;
+static StagePool g_stage_pool[kStageDevices];  // one per device, made on first use
 
-cudaError_t upload(void *dst, const void *src, size_t bytes, cudaStream_t s) {
-  if (bytes < 2 * kStageBytes)
-    return cudaMemcpyAsync(dst, src, bytes, cudaMemcpyHostToDevice, s);
-  cudaPointerAttributes at;
-  if (cudaPointerGetAttributes(&at, src) != cudaSuccess) {
-    cudaGetLastError();
-    at.type = cudaMemoryTypeUnregistered;
+// The networks' CSR arrays, for the SELL packing jobs of creation.
+struct PackSrc {
+  const int32_t *rp_cat, *col_cat;
+  const uint8_t *dl_cat;
+  const float *w_cat;
+  const std::vector<NetDesc> *nets;
+  const std::vector<long long> *sl_off;  // per slice, plus the total at the end
+  const std::vector<int> *sl_len;
+  const std::vector<int> *slice_net;     // network of each slice
+  int n_ext;                             // halo columns of network 0
+};
+
+struct StageJob {
+  int kind;              // 0: H2D copy, 1: SELL pack, 2: D2H copy
+  void *dst;             // copy: destination
+  const void *src;       // copy: source
+  size_t bytes;          // copy: size
+  long long s0, s1;      // pack: slices [s0, s1) ...
+  int k0, k1;            // ... and, for one slice in parts, entries k in [k0, k1)
+};
+
+// SELL-32 entries of slices [s0, s1) (for a part of one slice: entries
+// k0 <= k < k1) into cd[] and w[] (host), validating columns and delays:
+// bit 1 a column out of range, bit 2 a delay above max_delay, bit 4 a zero
+// delay.  Padding entries are node 0, delay 0, weight 0 (read, never used).
+unsigned pack_slices(const PackSrc &ps, long long s0, long long s1, int k0, int k1,
+                     uint32_t *cd, float *w) {
+  unsigned bad = 0u;
+  size_t o = 0;
+  for (long long s = s0; s < s1; ++s) {
+    const int n = (*ps.slice_net)[s];
+    const NetDesc &d = (*ps.nets)[n];
+    const int32_t *rp = ps.rp_cat + d.rp_off;
+    const int32_t *col = ps.col_cat + d.edge_off;
+    const uint8_t *dl = ps.dl_cat + d.edge_off;
+    const float *wv = ps.w_cat + d.edge_off;
+    const int ncols = d.N + (n == 0 ? ps.n_ext : 0);
+    const int row0 = (int)(s - d.slice_base) * 32;
+    const int len = (*ps.sl_len)[s];
+    const bool part = (k1 >= 0);
+    const int ka = part ? k0 : 0, kb = part ? k1 : len;
+    for (int l = 0; l < 32; ++l) {
+      const int row = row0 + l;
+      int e0 = 0, deg = 0;
+      if (row < d.N) {
+        e0 = rp[row];
+        deg = rp[row + 1] - e0;
+      }
+      const int kd = std::min(std::max(deg, ka), kb);
+      for (int k = ka; k < kd; ++k) {
+        const int c = col[e0 + k];
+        const unsigned de = dl[e0 + k];
+        if (c < 0 || c >= ncols) bad |= 1u;
+        if ((int)de > d.max_delay) bad |= 2u;
+        if (de == 0u) bad |= 4u;
+        cd[o + 32 * (size_t)(k - ka) + l] = ((uint32_t)c << 8) | de;
+        w[o + 32 * (size_t)(k - ka) + l] = wv[e0 + k];
+      }
+      for (int k = kd; k < kb; ++k) {
+        cd[o + 32 * (size_t)(k - ka) + l] = 0u;
+        w[o + 32 * (size_t)(k - ka) + l] = 0.0f;
+      }
+    }
+    o += 32 * (size_t)(kb - ka);
   }
-  if (at.type != cudaMemoryTypeUnregistered)
-    return cudaMemcpyAsync(dst, src, bytes, cudaMemcpyHostToDevice, s);
+  return bad;
+}
+
+// Runs the jobs on the staging threads; *bad receives the OR of the packing
+// jobs' validation bits.  H2D sources are fully read and D2H destinations
+// fully written when this returns (the H2D DMAs may still be in flight).
+cudaError_t run_stage_jobs(const std::vector<StageJob> &jobs, cudaStream_t s,
+                           const PackSrc *ps, uint32_t *d_cd, float *d_w, unsigned *bad) {
+  if (bad) *bad = 0u;
+  if (jobs.empty()) return cudaSuccess;
   int dev = 0;
   cudaError_t ce = cudaGetDevice(&dev);
   if (ce != cudaSuccess) return ce;
+  if (dev < 0 || dev >= kStageDevices) return cudaErrorInvalidDevice;
+  StagePool &g_stage = g_stage_pool[dev];
   std::lock_guard<std::mutex> lk(g_stage.mu);
-  if (g_stage.nbuf > 0 && g_stage.device != dev)  // the events belong to another device
-    return cudaMemcpyAsync(dst, src, bytes, cudaMemcpyHostToDevice, s);
   if (g_stage.nbuf == 0) {
-    g_stage.device = dev;
-    const unsigned hw = std::thread::hardware_concurrency();
-    const int want = (int)std::max(2u, std::min<unsigned>(kStageBufs, hw / 2));
-    for (int b = 0; b < want; ++b) {
-      if (cudaHostAlloc(&g_stage.buf[b], kStageBytes,
-                        cudaHostAllocPortable) != cudaSuccess ||
+    for (int b = 0; b < kStageBufs; ++b) {
+      if (cudaHostAlloc(&g_stage.buf[b], kStageBytes, cudaHostAllocPortable) != cudaSuccess ||
           cudaEventCreateWithFlags(&g_stage.ev[b], cudaEventDisableTiming) != cudaSuccess) {
         cudaGetLastError();
         if (g_stage.buf[b]) cudaFreeHost(g_stage.buf[b]);
         g_stage.buf[b] = nullptr;
         break;
       }
-      // a first wait on the event returns at once
-      cudaEventRecord(g_stage.ev[b], s);
+      cudaEventRecord(g_stage.ev[b], s);  // a first wait returns at once
       g_stage.nbuf = b + 1;
     }
-    if (g_stage.nbuf < 2) return cudaMemcpyAsync(dst, src, bytes, cudaMemcpyHostToDevice, s);
+    if (g_stage.nbuf < 2) return cudaErrorMemoryAllocation;
   }
-  const long long nchunks = (long long)((bytes + kStageBytes - 1) / kStageBytes);
+  const long long hw = std::max(2u, std::thread::hardware_concurrency());
+  const int nth = (int)std::min({(long long)g_stage.nbuf / 2, hw, (long long)jobs.size()});
+  const std::vector<long long> *sl_off = ps ? ps->sl_off : nullptr;
   std::atomic<long long> next{0};
   std::atomic<int> failed{(int)cudaSuccess};
-  auto worker = [&](int b) {
+  std::atomic<unsigned> bad_all{0u};
+  auto worker = [&](int t) {
     if (cudaSetDevice(dev) != cudaSuccess) {
       failed = (int)cudaErrorInvalidDevice;
       return;
     }
-    for (;;) {
-      const long long c = next++;
-      if (c >= nchunks || failed != (int)cudaSuccess) break;
-      const size_t off = (size_t)c * kStageBytes;
-      const size_t n = std::min(kStageBytes, bytes - off);
+    unsigned my_bad = 0u;
+    for (int turn = 0;; ++turn) {
+      const long long j = next++;
+      if (j >= (long long)jobs.size() || failed != (int)cudaSuccess) break;
+      const StageJob &job = jobs[j];
+      const int b = 2 * t + (turn & 1);
+      char *buf = static_cast<char *>(g_stage.buf[b]);
       cudaError_t e = cudaEventSynchronize(g_stage.ev[b]);  // its last DMA is done
-      if (e == cudaSuccess) {
-        std::memcpy(g_stage.buf[b], static_cast<const char *>(src) + off, n);
-        e = cudaMemcpyAsync(static_cast<char *>(dst) + off, g_stage.buf[b], n,
-                            cudaMemcpyHostToDevice, s);
+      if (e == cudaSuccess && job.kind == 0) {
+        std::memcpy(buf, job.src, job.bytes);
+        e = cudaMemcpyAsync(job.dst, buf, job.bytes, cudaMemcpyHostToDevice, s);
+      } else if (e == cudaSuccess && job.kind == 1) {
+        const long long first = (*sl_off)[job.s0] + (job.k1 >= 0 ? 32LL * job.k0 : 0);
+        const long long last = job.k1 >= 0 ? (*sl_off)[job.s0] + 32LL * job.k1
+                                           : (*sl_off)[job.s1];
+        const size_t n = (size_t)(last - first);
+        uint32_t *cd = reinterpret_cast<uint32_t *>(buf);
+        float *w = reinterpret_cast<float *>(buf + 4 * n);
+        my_bad |= pack_slices(*ps, job.s0, job.s1, job.k0, job.k1, cd, w);
+        e = cudaMemcpyAsync(d_cd + first, cd, 4 * n, cudaMemcpyHostToDevice, s);
+        if (e == cudaSuccess)
+          e = cudaMemcpyAsync(d_w + first, w, 4 * n, cudaMemcpyHostToDevice, s);
+      } else if (e == cudaSuccess && job.kind == 2) {
+        e = cudaMemcpyAsync(buf, job.src, job.bytes, cudaMemcpyDeviceToHost, s);
+        if (e == cudaSuccess) e = cudaEventRecord(g_stage.ev[b], s);
+        if (e == cudaSuccess) e = cudaEventSynchronize(g_stage.ev[b]);
+        if (e == cudaSuccess) std::memcpy(job.dst, buf, job.bytes);
       }
       if (e == cudaSuccess) e = cudaEventRecord(g_stage.ev[b], s);
       if (e != cudaSuccess) {
@@ -979,13 +1073,83 @@ cudaError_t upload(void *dst, const void *src, size_t bytes, cudaStream_t s) {
         break;
       }
     }
+    bad_all |= my_bad;
   };
-  const int nth = (int)std::min<long long>(g_stage.nbuf, nchunks);
   std::vector<std::thread> th;
-  for (int b = 1; b < nth; ++b) th.emplace_back(worker, b);
+  for (int t = 1; t < nth; ++t) th.emplace_back(worker, t);
   worker(0);
-  for (auto &t : th) t.join();
+  for (auto &x : th) x.join();
+  if (bad) *bad = bad_all.load();
   return (cudaError_t)failed.load();
+}
+
+// Copy jobs of at most kStageBytes for one array (kind 0: H2D, 2: D2H).
+void add_copy_jobs(std::vector<StageJob> &jobs, int kind, void *dst, const void *src,
+                   size_t bytes) {
+  for (size_t off = 0; off < bytes; off += kStageBytes) {
+    StageJob j{};
+    j.kind = kind;
+    j.dst = static_cast<char *>(dst) + off;
+    j.src = static_cast<const char *>(src) + off;
+    j.bytes = std::min(kStageBytes, bytes - off);
+    j.k1 = -1;
+    jobs.push_back(j);
+  }
+}
+
+// SELL packing jobs over all slices: runs of whole slices of at most
+// kStageBytes / 8 entries (cd and w of an entry: 8 bytes), or parts of one
+// slice that is larger than that.  sl_off holds one more entry, the total.
+void add_pack_jobs(std::vector<StageJob> &jobs, const std::vector<long long> &sl_off,
+                   const std::vector<int> &sl_len, long long slices) {
+  const long long cap = (long long)(kStageBytes / 8);
+  long long s = 0;
+  while (s < slices) {
+    if (32LL * sl_len[s] > cap) {  // one large slice, in parts
+      const int step = (int)(cap / 32);
+      for (int k0 = 0; k0 < sl_len[s]; k0 += step) {
+        StageJob j{};
+        j.kind = 1;
+        j.s0 = s;
+        j.s1 = s + 1;
+        j.k0 = k0;
+        j.k1 = std::min(sl_len[s], k0 + step);
+        jobs.push_back(j);
+      }
+      ++s;
+      continue;
+    }
+    long long e = s;
+    while (e < slices && 32LL * sl_len[e] <= cap && sl_off[e + 1] - sl_off[s] <= cap) ++e;
+    StageJob j{};
+    j.kind = 1;
+    j.s0 = s;
+    j.s1 = e;
+    j.k0 = 0;
+    j.k1 = -1;
+    if (sl_off[e] > sl_off[s]) jobs.push_back(j);
+    s = e;
+  }
+}
+
+// Staged host -> device copy of one array.
+cudaError_t upload(void *dst, const void *src, size_t bytes, cudaStream_t s) {
+  if (bytes < 2 * kStageBytes) return cudaMemcpyAsync(dst, src, bytes, cudaMemcpyHostToDevice, s);
+  std::vector<StageJob> jobs;
+  add_copy_jobs(jobs, 0, dst, src, bytes);
+  return run_stage_jobs(jobs, s, nullptr, nullptr, nullptr, nullptr);
+}
+
+// Staged device -> host copy into caller (pageable) memory; synchronous.
+cudaError_t download(void *dst, const void *src, size_t bytes, cudaStream_t s) {
+  if (bytes < 2 * kStageBytes) {
+    cudaError_t e = cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDeviceToHost, s);
+    return e == cudaSuccess ? cudaStreamSynchronize(s) : e;
+  }
+  std::vector<StageJob> jobs;
+  add_copy_jobs(jobs, 2, dst, const_cast<void *>(src), bytes);
+  cudaError_t e = cudaStreamSynchronize(s);  // the data is complete on the device
+  return e == cudaSuccess ? run_stage_jobs(jobs, s, nullptr, nullptr, nullptr, nullptr) : e;
 }
 
 // Every ring slot of halo columns N .. N + n_ext - 1 of network 0 := the
@@ -1137,6 +1301,13 @@ int create_impl(LevEngine **out, int num_nets, const int32_t *Ns,
     delete h;
     return fail(LEV_ERR_ARG, "null edge array argument");
   }
+  h_sl_off.push_back(sl_total);  // end of the last slice (packing jobs)
+  std::vector<int> slice_net((size_t)slices);
+  for (int n = 0; n < num_nets; ++n) {
+    const NetDesc &d = h->h_nets[n];
+    const long long ns = (d.N + 31) / 32;
+    for (long long k = 0; k < ns; ++k) slice_net[(size_t)(d.slice_base + k)] = n;
+  }
   h->total_nodes = node_off;
   h->total_edges = edge_off;
   h->num_slices = slices;
@@ -1220,25 +1391,49 @@ int create_impl(LevEngine **out, int num_nets, const int32_t *Ns,
       if (!ok) rc = fail(LEV_ERR_CUDA, "class streams: creation failed");
     }
   }
-#define LEV_ALLOC(ptr, count)                      \
-  if (rc == LEV_OK) rc = dev_alloc(h, &(ptr), (count));
-  LEV_ALLOC(h->d_nets, (size_t)num_nets);
-  LEV_ALLOC(h->d_st, (size_t)num_nets);
-  LEV_ALLOC(h->d_tiles, (size_t)tiles);
-  LEV_ALLOC(h->d_row_ptr, (size_t)rp_off);
-  LEV_ALLOC(h->d_sl_off, (size_t)slices);
-  LEV_ALLOC(h->d_sl_len, (size_t)slices);
-  LEV_ALLOC(h->d_sl_cd, (size_t)sl_total);
-  LEV_ALLOC(h->d_sl_w, (size_t)sl_total);
-  LEV_ALLOC(h->d_theta, (size_t)node_off);
-  LEV_ALLOC(h->d_theta_hat, (size_t)node_off);
-  LEV_ALLOC(h->d_omega, (size_t)node_off);
-  LEV_ALLOC(h->d_omega_hat, (size_t)node_off);
-  LEV_ALLOC(h->d_ring, (size_t)ring_off);
-  LEV_ALLOC(h->d_part, (size_t)tiles);
-  LEV_ALLOC(h->d_rhist, (size_t)h->block_len * num_nets);
-  LEV_ALLOC(h->d_class_nets, (size_t)num_nets);
-#undef LEV_ALLOC
+  // every array sized here in one device allocation (256-byte aligned
+  // parts): one cudaMalloc instead of one per array
+  {
+    struct Part { void **p; size_t bytes; };
+    const Part parts[] = {
+        {(void **)&h->d_nets, sizeof(NetDesc) * num_nets},
+        {(void **)&h->d_st, sizeof(NetState) * num_nets},
+        {(void **)&h->d_tiles, sizeof(int2) * std::max(tiles, 1)},
+        {(void **)&h->d_row_ptr, sizeof(int) * rp_off},
+        {(void **)&h->d_sl_off, sizeof(long long) * std::max<long long>(slices, 1)},
+        {(void **)&h->d_sl_len, sizeof(int) * std::max<long long>(slices, 1)},
+        {(void **)&h->d_sl_cd, sizeof(uint32_t) * std::max<long long>(sl_total, 1)},
+        {(void **)&h->d_sl_w, sizeof(float) * std::max<long long>(sl_total, 1)},
+        {(void **)&h->d_theta, sizeof(float) * node_off},
+        {(void **)&h->d_theta_hat, sizeof(float) * node_off},
+        {(void **)&h->d_omega, sizeof(float) * node_off},
+        {(void **)&h->d_omega_hat, sizeof(float) * node_off},
+        {(void **)&h->d_ring, sizeof(float) * ring_off},
+        {(void **)&h->d_part, sizeof(float2) * std::max(tiles, 1)},
+        {(void **)&h->d_rhist, sizeof(float) * h->block_len * num_nets},
+        {(void **)&h->d_class_nets, sizeof(int) * num_nets},
+        {(void **)&h->d_pend, sizeof(float2) * node_off},
+    };
+    size_t total = 0;
+    for (const Part &q : parts) total += (q.bytes + 255) / 256 * 256;
+    if (rc == LEV_OK) {
+      cudaError_t e = cudaMalloc(&h->slab, total);
+      if (e != cudaSuccess) {
+        h->slab = nullptr;
+        rc = fail(LEV_ERR_NOMEM, std::string("cudaMalloc of ") + std::to_string(total) +
+                                     " bytes failed: " + cudaGetErrorString(e));
+      }
+    }
+    if (rc == LEV_OK) {
+      h->slab_bytes = total;
+      h->vram += total;
+      char *c = static_cast<char *>(h->slab);
+      for (const Part &q : parts) {
+        *q.p = c;
+        c += (q.bytes + 255) / 256 * 256;
+      }
+    }
+  }
   if (rc != LEV_OK) {
     std::string msg = g_last_error;
     free_engine(h);
@@ -1256,35 +1451,14 @@ int create_impl(LevEngine **out, int num_nets, const int32_t *Ns,
   }
 
   mark(1);
-  // ---- uploads -------------------------------------------------------------
-  unsigned *d_err = nullptr;
-  uint8_t *d_tmp = nullptr;    // delays, CSR order
-  int *d_tcol = nullptr;       // col_idx, CSR order
-  float *d_tw = nullptr;       // weights, CSR order
+  // ---- uploads: one staged pass over the caller's arrays -------------------
+  // (edges are packed into SELL-32 on the host, in the staging buffers, and
+  // validated there; the node arrays are copied through the same buffers)
   auto cleanup_fail = [&](int code, const std::string &msg) {
-    if (d_err) cudaFree(d_err);
-    if (d_tmp) cudaFree(d_tmp);
-    if (d_tcol) cudaFree(d_tcol);
-    if (d_tw) cudaFree(d_tw);
+    cudaStreamSynchronize(h->stream);
     free_engine(h);
     return fail(code, msg);
   };
-#define LEV_UP(dst, src, bytes)                                            \
-  do {                                                                     \
-    cudaError_t _e = upload((dst), (src), (bytes), h->stream);             \
-    if (_e != cudaSuccess)                                                 \
-      return cleanup_fail(LEV_ERR_CUDA, std::string("upload failed: ") +   \
-                                            cudaGetErrorString(_e));       \
-  } while (0)
-  LEV_UP(h->d_nets, h->h_nets.data(), sizeof(NetDesc) * num_nets);
-  LEV_UP(h->d_tiles, h_tiles.data(), sizeof(int2) * tiles);
-  LEV_UP(h->d_class_nets, h_class_nets.data(), sizeof(int) * num_nets);
-  LEV_UP(h->d_row_ptr, rp_cat, sizeof(int32_t) * rp_off);
-  LEV_UP(h->d_theta, th_cat, sizeof(float) * node_off);
-  LEV_UP(h->d_theta_hat, thh_cat, sizeof(float) * node_off);
-  LEV_UP(h->d_omega, om_cat, sizeof(float) * node_off);
-  // omega_hat starts as omega (leviathan_kernel.cu:350)
-  LEV_UP(h->d_omega_hat, om_cat, sizeof(float) * node_off);
   std::vector<NetState> st(num_nets);
   for (int n = 0; n < num_nets; ++n) {
     std::memset(&st[n], 0, sizeof(NetState));
@@ -1292,76 +1466,45 @@ int create_impl(LevEngine **out, int num_nets, const int32_t *Ns,
     if (params) p = params[n]; else lev_default_params(&p);
     st[n].g = p.g;
   }
-  LEV_UP(h->d_st, st.data(), sizeof(NetState) * num_nets);
-  LEV_UP(h->d_sl_off, h_sl_off.data(), sizeof(long long) * slices);
-  LEV_UP(h->d_sl_len, h_sl_len.data(), sizeof(int) * slices);
-  // padding entries: node 0, delay 0, weight 0 (read, never used)
-  if (cudaMemsetAsync(h->d_sl_cd, 0, sizeof(uint32_t) * std::max<long long>(sl_total, 1),
-                      h->stream) != cudaSuccess ||
-      cudaMemsetAsync(h->d_sl_w, 0, sizeof(float) * std::max<long long>(sl_total, 1),
-                      h->stream) != cudaSuccess ||
-      cudaMemsetAsync(h->d_ring, 0, sizeof(float) * std::max<long long>(ring_off, 1),
-                      h->stream) != cudaSuccess)
-    return cleanup_fail(LEV_ERR_CUDA, "memset failed");
-
+  {
+    cudaError_t e = cudaMemsetAsync(h->d_ring, 0, sizeof(float) * std::max<long long>(ring_off, 1),
+                                    h->stream);
+    const struct { void *dst; const void *src; size_t bytes; } small[] = {
+        {h->d_nets, h->h_nets.data(), sizeof(NetDesc) * num_nets},
+        {h->d_tiles, h_tiles.data(), sizeof(int2) * tiles},
+        {h->d_class_nets, h_class_nets.data(), sizeof(int) * num_nets},
+        {h->d_st, st.data(), sizeof(NetState) * num_nets},
+        {h->d_sl_off, h_sl_off.data(), sizeof(long long) * slices},
+        {h->d_sl_len, h_sl_len.data(), sizeof(int) * slices},
+    };
+    for (const auto &c : small)
+      if (e == cudaSuccess && c.bytes > 0)
+        e = cudaMemcpyAsync(c.dst, c.src, c.bytes, cudaMemcpyHostToDevice, h->stream);
+    if (e != cudaSuccess)
+      return cleanup_fail(LEV_ERR_CUDA, std::string("upload failed: ") + cudaGetErrorString(e));
+  }
   mark(2);
-  if (edge_off > 0) {
-    if (cudaMalloc(&d_tmp, edge_off) != cudaSuccess ||
-        cudaMalloc(&d_tcol, sizeof(int) * edge_off) != cudaSuccess ||
-        cudaMalloc(&d_tw, sizeof(float) * edge_off) != cudaSuccess ||
-        cudaMalloc(&d_err, sizeof(unsigned)) != cudaSuccess)
-      return cleanup_fail(LEV_ERR_NOMEM, "temporary upload buffer");
-    LEV_UP(d_tw, w_cat, sizeof(float) * edge_off);
-    LEV_UP(d_tcol, col_cat, sizeof(int32_t) * edge_off);
-    LEV_UP(d_tmp, d_cat, edge_off);
-    if (cudaMemsetAsync(d_err, 0, sizeof(unsigned), h->stream) != cudaSuccess)
-      return cleanup_fail(LEV_ERR_CUDA, "memset failed");
+  {
+    std::vector<StageJob> jobs;
+    add_copy_jobs(jobs, 0, h->d_row_ptr, rp_cat, sizeof(int32_t) * rp_off);
+    add_copy_jobs(jobs, 0, h->d_theta, th_cat, sizeof(float) * node_off);
+    add_copy_jobs(jobs, 0, h->d_theta_hat, thh_cat, sizeof(float) * node_off);
+    add_copy_jobs(jobs, 0, h->d_omega, om_cat, sizeof(float) * node_off);
+    // omega_hat starts as omega (leviathan_kernel.cu:350)
+    add_copy_jobs(jobs, 0, h->d_omega_hat, om_cat, sizeof(float) * node_off);
+    add_pack_jobs(jobs, h_sl_off, h_sl_len, slices);
+    PackSrc ps{rp_cat, col_cat, d_cat, w_cat, &h->h_nets, &h_sl_off, &h_sl_len, &slice_net,
+               n_ext};
+    unsigned herr = 0u;
+    cudaError_t e = run_stage_jobs(jobs, h->stream, &ps, h->d_sl_cd, h->d_sl_w, &herr);
+    if (e != cudaSuccess)
+      return cleanup_fail(LEV_ERR_CUDA, std::string("upload failed: ") + cudaGetErrorString(e));
     mark(3);
-    for (int n = 0; n < num_nets; ++n) {
-      const NetDesc &d = h->h_nets[n];
-      if (h->net_E[n] == 0) continue;
-      int blocks = (int)std::min<long long>((d.N + 255) / 256, 148LL * 16);
-      sell_convert_kernel<<<blocks, 256, 0, h->stream>>>(
-          0, h->d_row_ptr + d.rp_off, d.N, d.N + n_ext, d.slice_base, h->d_sl_off,
-          d_tcol + d.edge_off, d_tmp + d.edge_off, d_tw + d.edge_off,
-          h->d_sl_cd, h->d_sl_w, d.max_delay, d_err);
-    }
-    unsigned herr = 0;
-    cudaError_t e1 = cudaGetLastError();
-    cudaError_t e2 = cudaMemcpyAsync(&herr, d_err, sizeof(unsigned),
-                                     cudaMemcpyDeviceToHost, h->stream);
-    cudaError_t e3 = cudaStreamSynchronize(h->stream);
-    if (e1 != cudaSuccess || e2 != cudaSuccess || e3 != cudaSuccess)
-      return cleanup_fail(LEV_ERR_CUDA,
-                          std::string("edge packing failed: ") +
-                              cudaGetErrorString(e1 != cudaSuccess ? e1
-                                                 : e2 != cudaSuccess ? e2
-                                                                     : e3));
-    if (herr & 1u)
-      return cleanup_fail(LEV_ERR_ARG, "col_idx out of range [0, N)");
-    if (herr & 2u)
-      return cleanup_fail(LEV_ERR_ARG, "delay larger than max_delay");
+    if (herr & 1u) return cleanup_fail(LEV_ERR_ARG, "col_idx out of range [0, N)");
+    if (herr & 2u) return cleanup_fail(LEV_ERR_ARG, "delay larger than max_delay");
     h->pair_ok = !(herr & 4u);
-    mark(4);
-    cudaFree(d_tmp);
-    cudaFree(d_tcol);
-    cudaFree(d_tw);
-    cudaFree(d_err);
-    d_tmp = nullptr;
-    d_tcol = nullptr;
-    d_tw = nullptr;
-    d_err = nullptr;
   }
-#undef LEV_UP
-  if (edge_off == 0) h->pair_ok = true;
-  if (h->pair_ok) {
-    int r2 = dev_alloc(h, &h->d_pend, (size_t)node_off);
-    if (r2 != LEV_OK) {
-      std::string msg = g_last_error;
-      free_engine(h);
-      return fail(r2, msg);
-    }
-  }
+  mark(4);
   for (int n = 0; n < num_nets; ++n) {
     int r2 = launch_fill(h, n);
     if (r2 != LEV_OK) {
@@ -1589,16 +1732,13 @@ int lev_get_stream(LevEngine *h, void **stream) {
 
 static int copy_nodes(LevEngine *h, float *dst_host, const float *src_dev,
                       long long off, long long count) {
-  LEV_TRY_CUDA(cudaMemcpyAsync(dst_host, src_dev + off, sizeof(float) * count,
-                               cudaMemcpyDeviceToHost, h->stream));
-  LEV_TRY_CUDA(cudaStreamSynchronize(h->stream));
+  LEV_TRY_CUDA(download(dst_host, src_dev + off, sizeof(float) * count, h->stream));
   return LEV_OK;
 }
 
 static int upload_nodes(LevEngine *h, float *dst_dev, const float *src_host,
                         long long off, long long count) {
-  LEV_TRY_CUDA(cudaMemcpyAsync(dst_dev + off, src_host, sizeof(float) * count,
-                               cudaMemcpyHostToDevice, h->stream));
+  LEV_TRY_CUDA(upload(dst_dev + off, src_host, sizeof(float) * count, h->stream));
   return LEV_OK;
 }
 
