@@ -122,10 +122,13 @@ int lev_batch_create(LevEngine **out, int32_t num_nets, const int32_t *N,
 int lev_destroy(LevEngine *h);
 
 /* Wall-clock milliseconds of the phases of the engine's creation (no
- * reference counterpart; for tuning construction): ms_out[6] = host-side
- * validation and layout, device resources (stream, allocations), node-array
- * uploads, edge-array uploads (host side), CSR -> SELL conversion (waits for
- * the uploads), ring fill and the final synchronisation. */
+ * reference counterpart; for tuning construction): ms_out[8] = host-side
+ * validation and layout; stream and kernel set-up; the one device
+ * allocation; the mapped host buffer of r; small uploads (descriptors, tile
+ * lists); the staged pass over the caller's arrays (host threads pack the
+ * edges into SELL-32 and copy the node arrays into pinned buffers,
+ * validating columns and delays, and issue the DMAs); the ring-fill launch;
+ * the wait for every DMA and the fill. */
 int lev_create_profile(const LevEngine *h, double *ms_out);
 
 /* Shape queries. */
@@ -303,6 +306,11 @@ int lev_set_grid_wait(LevEngine *h, uint64_t limit_ns, uint32_t extra_arrivals);
 int lev_num_pair_variants(void);
 int lev_pair_variant_info(int32_t v, int32_t *unroll, int32_t *min_blocks,
                           int32_t *deep);
+/* Threads per row of pair variant v (1, or 4: the row's SELL entries split
+ * over four lanes, for low-degree networks; the coupling sum is formed in
+ * CSR order from the four lanes' terms, bitwise as with one lane).  The
+ * autotuner searches this dimension with the others, per degree class. */
+int lev_pair_variant_lanes(int32_t v, int32_t *lanes);
 int lev_pair_info(const LevEngine *h, int32_t c, int32_t *eligible, int32_t *enabled,
                   int32_t *pair_variant, float *pair_ms, float *step_ms);
 int lev_set_pair_mode(LevEngine *h, int32_t enabled);

@@ -109,6 +109,7 @@ PROTOTYPES = {
     "lev_num_pair_variants": (C.c_int, []),
     "lev_pair_variant_info": (C.c_int, [_i32, C.POINTER(_i32), C.POINTER(_i32),
                                         C.POINTER(_i32)]),
+    "lev_pair_variant_lanes": (C.c_int, [_i32, C.POINTER(_i32)]),
     "lev_pair_info": (C.c_int, [_P, _i32, C.POINTER(_i32), C.POINTER(_i32),
                                 C.POINTER(_i32), C.POINTER(_f32), C.POINTER(_f32)]),
     "lev_set_pair_mode": (C.c_int, [_P, _i32]),

@@ -86,17 +86,23 @@ constexpr int kNumVariants = sizeof(kVariants) / sizeof(kVariants[0]);
 // resident CTAs with more loads in flight per lane win at large networks
 // (the L1 keeps the tile's ring lines and col/delay words between the two
 // walks); more CTAs win at the small networks of a sweep.
+// LANES: threads per row (1: pair_kernel, 256-thread CTAs; 4: pair4_kernel,
+// 1024-thread CTAs for low-degree rows).
 struct PairVariant {
-  int U, MINB, DEEP;
+  int U, MINB, DEEP, LANES;
   StepFn fn[2];  // [math mode]
 };
 #define LEV_PAIR_VARIANT(U, M, D) \
-  { U, M, D, { pair_kernel<0, U, M, D>, pair_kernel<1, U, M, D> } }
+  { U, M, D, 1, { pair_kernel<0, U, M, D>, pair_kernel<1, U, M, D> } }
+#define LEV_PAIR4_VARIANT(U, M) \
+  { U, M, 0, 4, { pair4_kernel<0, U, M>, pair4_kernel<1, U, M> } }
 static const PairVariant kPairVariants[] = {
     LEV_PAIR_VARIANT(8, 2, 1), LEV_PAIR_VARIANT(6, 3, 1), LEV_PAIR_VARIANT(8, 3, 0),
-    LEV_PAIR_VARIANT(4, 4, 1), LEV_PAIR_VARIANT(10, 2, 1),
+    LEV_PAIR_VARIANT(4, 4, 1), LEV_PAIR_VARIANT(10, 2, 1), LEV_PAIR4_VARIANT(2, 1),
+    LEV_PAIR4_VARIANT(4, 1),
 };
 #undef LEV_PAIR_VARIANT
+#undef LEV_PAIR4_VARIANT
 constexpr int kNumPairVariants = sizeof(kPairVariants) / sizeof(kPairVariants[0]);
 
 // Networks of a batch are grouped by the mean SELL slice length (the
@@ -231,7 +237,7 @@ struct LevEngine {
   size_t slab_bytes = 0;
 
   // wall-clock ms of the phases of creation (lev_create_profile)
-  double create_ms[6] = {0, 0, 0, 0, 0, 0};
+  double create_ms[8] = {0, 0, 0, 0, 0, 0, 0, 0};
 
   // partition of a network split over GPUs (lev_part.cuh, lev_part_*): own
   // rows stepped here, halo phases in ring columns N .. N + part_halo - 1
@@ -483,8 +489,9 @@ int launch_pair_class(LevEngine *h, int c, StepArgs a, int phase, cudaStream_t s
         tc.pair_variant < 0
             ? reinterpret_cast<const void *>(kVariants[tc.variant].fn[mode])
             : reinterpret_cast<const void *>(kPairVariants[tc.pair_variant].fn[mode]);
+    const int lanes = tc.pair_variant < 0 ? 1 : kPairVariants[tc.pair_variant].LANES;
     void *args[] = {&a};
-    LEV_TRY_CUDA(cudaLaunchKernel(fn, dim3(tc.ntiles), dim3(kTile), args, 0, s));
+    LEV_TRY_CUDA(cudaLaunchKernel(fn, dim3(tc.ntiles), dim3(lanes * kTile), args, 0, s));
   } else {
     const int blocks = (tc.ntiles + kFinishTiles - 1) / kFinishTiles;
     if (mode)
@@ -1083,15 +1090,17 @@ cudaError_t run_stage_jobs(const std::vector<StageJob> &jobs, cudaStream_t s,
   return (cudaError_t)failed.load();
 }
 
-// Copy jobs of at most kStageBytes for one array (kind 0: H2D, 2: D2H).
+// Copy jobs of at most `chunk` (<= kStageBytes) bytes for one array (kind 0:
+// H2D, 2: D2H).
 void add_copy_jobs(std::vector<StageJob> &jobs, int kind, void *dst, const void *src,
-                   size_t bytes) {
-  for (size_t off = 0; off < bytes; off += kStageBytes) {
+                   size_t bytes, size_t chunk = kStageBytes) {
+  chunk = std::min(chunk, kStageBytes);
+  for (size_t off = 0; off < bytes; off += chunk) {
     StageJob j{};
     j.kind = kind;
     j.dst = static_cast<char *>(dst) + off;
     j.src = static_cast<const char *>(src) + off;
-    j.bytes = std::min(kStageBytes, bytes - off);
+    j.bytes = std::min(chunk, bytes - off);
     j.k1 = -1;
     jobs.push_back(j);
   }
@@ -1141,13 +1150,17 @@ cudaError_t upload(void *dst, const void *src, size_t bytes, cudaStream_t s) {
 }
 
 // Staged device -> host copy into caller (pageable) memory; synchronous.
+// Arrays from 512 KiB on are cut into at least eight chunks, so that the
+// copies out of the pinned buffers (and the first-touch page faults of a
+// fresh destination) run on several host threads.
 cudaError_t download(void *dst, const void *src, size_t bytes, cudaStream_t s) {
-  if (bytes < 2 * kStageBytes) {
+  if (bytes < (512u << 10)) {
     cudaError_t e = cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDeviceToHost, s);
     return e == cudaSuccess ? cudaStreamSynchronize(s) : e;
   }
   std::vector<StageJob> jobs;
-  add_copy_jobs(jobs, 2, dst, const_cast<void *>(src), bytes);
+  const size_t chunk = std::max<size_t>(64u << 10, (bytes / 8 + 4095) / 4096 * 4096);
+  add_copy_jobs(jobs, 2, dst, const_cast<void *>(src), bytes, chunk);
   cudaError_t e = cudaStreamSynchronize(s);  // the data is complete on the device
   return e == cudaSuccess ? run_stage_jobs(jobs, s, nullptr, nullptr, nullptr, nullptr) : e;
 }
@@ -1391,6 +1404,7 @@ int create_impl(LevEngine **out, int num_nets, const int32_t *Ns,
       if (!ok) rc = fail(LEV_ERR_CUDA, "class streams: creation failed");
     }
   }
+  mark(1);
   // every array sized here in one device allocation (256-byte aligned
   // parts): one cudaMalloc instead of one per array
   {
@@ -1439,6 +1453,7 @@ int create_impl(LevEngine **out, int num_nets, const int32_t *Ns,
     free_engine(h);
     return fail(rc, msg);
   }
+  mark(2);
   ce = cudaHostAlloc(reinterpret_cast<void **>(&h->h_rmap),
                      sizeof(float) * num_nets, cudaHostAllocMapped);
   if (ce == cudaSuccess)
@@ -1450,7 +1465,7 @@ int create_impl(LevEngine **out, int num_nets, const int32_t *Ns,
                                   cudaGetErrorString(ce));
   }
 
-  mark(1);
+  mark(3);
   // ---- uploads: one staged pass over the caller's arrays -------------------
   // (edges are packed into SELL-32 on the host, in the staging buffers, and
   // validated there; the node arrays are copied through the same buffers)
@@ -1483,7 +1498,7 @@ int create_impl(LevEngine **out, int num_nets, const int32_t *Ns,
     if (e != cudaSuccess)
       return cleanup_fail(LEV_ERR_CUDA, std::string("upload failed: ") + cudaGetErrorString(e));
   }
-  mark(2);
+  mark(4);
   {
     std::vector<StageJob> jobs;
     add_copy_jobs(jobs, 0, h->d_row_ptr, rp_cat, sizeof(int32_t) * rp_off);
@@ -1499,12 +1514,11 @@ int create_impl(LevEngine **out, int num_nets, const int32_t *Ns,
     cudaError_t e = run_stage_jobs(jobs, h->stream, &ps, h->d_sl_cd, h->d_sl_w, &herr);
     if (e != cudaSuccess)
       return cleanup_fail(LEV_ERR_CUDA, std::string("upload failed: ") + cudaGetErrorString(e));
-    mark(3);
+    mark(5);
     if (herr & 1u) return cleanup_fail(LEV_ERR_ARG, "col_idx out of range [0, N)");
     if (herr & 2u) return cleanup_fail(LEV_ERR_ARG, "delay larger than max_delay");
     h->pair_ok = !(herr & 4u);
   }
-  mark(4);
   for (int n = 0; n < num_nets; ++n) {
     int r2 = launch_fill(h, n);
     if (r2 != LEV_OK) {
@@ -1513,6 +1527,7 @@ int create_impl(LevEngine **out, int num_nets, const int32_t *Ns,
       return fail(r2, msg);
     }
   }
+  mark(6);
   if (n_ext > 0) {
     int r2 = fill_ext_columns(h, n_ext, theta_ext);
     if (r2 != LEV_OK) {
@@ -1527,7 +1542,7 @@ int create_impl(LevEngine **out, int num_nets, const int32_t *Ns,
     return fail(LEV_ERR_CUDA,
                 std::string("engine init failed: ") + cudaGetErrorString(ce));
   }
-  mark(5);
+  mark(7);
   *out = h;
   return LEV_OK;
 }
@@ -2132,7 +2147,7 @@ int lev_set_grid_wait(LevEngine *h, uint64_t limit_ns, uint32_t extra_arrivals) 
 
 int lev_create_profile(const LevEngine *h, double *ms_out) {
   if (!h || !ms_out) return fail(LEV_ERR_ARG, "null argument");
-  for (int k = 0; k < 6; ++k) ms_out[k] = h->create_ms[k];
+  for (int k = 0; k < 8; ++k) ms_out[k] = h->create_ms[k];
   return LEV_OK;
 }
 
@@ -2146,6 +2161,12 @@ int lev_pair_variant_info(int32_t v, int32_t *unroll, int32_t *min_blocks,
   if (unroll) *unroll = kPairVariants[v].U;
   if (min_blocks) *min_blocks = kPairVariants[v].MINB;
   if (deep) *deep = kPairVariants[v].DEEP;
+  return LEV_OK;
+}
+
+int lev_pair_variant_lanes(int32_t v, int32_t *lanes) {
+  if (v < 0 || v >= kNumPairVariants || !lanes) return fail(LEV_ERR_ARG, "bad pair variant");
+  *lanes = kPairVariants[v].LANES;
   return LEV_OK;
 }
 

@@ -357,6 +357,200 @@ __global__ void __launch_bounds__(kTile, MINB) pair_kernel(const StepArgs a) {
   tile_partial(a, nd, row0, my_cos, my_sin, s_rc, s_rs);
 }
 
+// ---------------------------------------------------------------------------
+// Four lanes per row: the threads-per-row dimension of the autotuner.  A row
+// of a low-degree network is only a few SELL entries long, so one lane per
+// row leaves most of the gathers' latency exposed; four lanes per row keep
+// four times as many rows' loads in flight per SM.  CTA = 1024 threads = one
+// 256-row tile (the same tiles and tile partials as pair_kernel); warp w
+// holds rows 8w .. 8w+7 of the tile, lane 4r + q of the warp is lane q of
+// row r, and lane q takes the row's SELL entries q, q+4, q+8, ...  Eight
+// rows' entries k are 32 contiguous bytes of the slice, so every stream load
+// of a warp is four full 32-byte sectors.  Each entry's arithmetic is that of
+// row_walk; the row's first lane forms the coupling sum in CSR order from the
+// other lanes' terms (shuffled to it in entry order), with the same fused
+// multiply-add, so the sum -- and the whole trajectory -- is bitwise that of
+// one lane per row.
+// ---------------------------------------------------------------------------
+template <int MATH, int U, int SECOND>
+__device__ __forceinline__ float row_walk4(const uint32_t *__restrict__ cdp,
+                                           float *wp, float *wo, int len, int deg,
+                                           const float *__restrict__ ring, int base,
+                                           int bsi, int Np, float th, float my_eps,
+                                           float dt, const NetDesc &nd, int q, int lead) {
+  const float eta = nd.eta, gamma = nd.gamma, lam = nd.lam;
+  const float w_min = nd.w_min, w_max = nd.w_max;
+  const unsigned mask = 0xffffffffu;
+  float local_sum = 0.0f;
+  for (int kb = 0; kb < len; kb += 4 * U) {  // len: the slice's, warp-uniform
+    uint32_t p[U];
+    float wv[U], dj[U], sn[U];
+#pragma unroll
+    for (int u = 0; u < U; ++u) {
+      const int k = kb + 4 * u + q;
+      if (SECOND) {
+        p[u] = (k < deg) ? __ldcs(cdp + 32 * k) : 0u;
+        wv[u] = (k < deg) ? __ldcs(wp + 32 * k) : 0.0f;
+      } else {
+        p[u] = (k < deg) ? __ldg(cdp + 32 * k) : 0u;
+        wv[u] = (k < deg) ? __ldcg(wp + 32 * k) : 0.0f;
+      }
+    }
+#pragma unroll
+    for (int u = 0; u < U; ++u) {
+      int slot = base - (int)(p[u] & 255u);
+      slot += (slot < 0) ? bsi : 0;
+      const float *src = ring + ((unsigned)slot * (unsigned)Np + (p[u] >> 8));
+      dj[u] = (kb + 4 * u + q < deg) ? ld_ring(src) : 0.0f;
+    }
+#pragma unroll
+    for (int u = 0; u < U; ++u) {
+      const int k = kb + 4 * u + q;
+      sn[u] = 0.0f;
+      if (k < deg) {
+        const float delayed_j = dj[u];
+        float diff = delayed_j - th;
+        diff = wrap_pm_pi(diff);
+        float w = wv[u];
+        float sin_diff, cos_diff;
+        lev_sincos<MATH>(diff, &sin_diff, &cos_diff);
+        sn[u] = sin_diff;
+        float dw = dt * (eta * cos_diff * (1.0f - gamma * my_eps) - lam * w);
+        w += dw;
+        if (!isfinite(w)) w = w_min;
+        w = fmaxf(w_min, fminf(w_max, w));
+        if (SECOND)
+          __stcs(wo + 32 * k, w);
+        else
+          __stcg(wp + 32 * k, w);
+      }
+    }
+    // the row sum in CSR order on the row's first lane (entry kb + e is
+    // lane e % 4's slot e / 4)
+#pragma unroll
+    for (int e = 0; e < 4 * U; ++e) {
+      const int src = lead + (e & 3);
+      const float w = __shfl_sync(mask, wv[e >> 2], src);
+      const float sin_diff = __shfl_sync(mask, sn[e >> 2], src);
+      if (kb + e < deg) local_sum += w * sin_diff;
+    }
+  }
+  return local_sum;
+}
+
+template <int MATH, int U, int MINB>
+__global__ void __launch_bounds__(4 * kTile, MINB) pair4_kernel(const StepArgs a) {
+  __shared__ float s_rc[32];
+  __shared__ float s_rs[32];
+  __shared__ float s_oc[kTile];
+  __shared__ float s_os[kTile];
+
+  const int tid = threadIdx.x;
+  const int lane = tid & 31, warp = tid >> 5;
+  const int q = lane & 3, lead = lane & ~3;
+  const int rloc = 8 * warp + (lane >> 2);  // row within the tile
+  const unsigned mask = 0xffffffffu;
+  const int tix = a.reverse ? (int)(gridDim.x - 1 - blockIdx.x) : (int)blockIdx.x;
+  const int2 tile = a.tiles[tix];
+  const NetDesc nd = a.nets[tile.x];
+  NetState *ns = a.st + tile.x;
+
+  const int N = nd.N;
+  const int row0 = tile.y;
+  const int row = row0 + rloc;
+  const bool live = row < N;
+  const long long gi = nd.node_off + row;
+  const float dt = a.dt;
+  const int bsi = nd.bsi;
+  const int Np = nd.Np;
+  const int cur = ns->cur;
+  const int nxt = nxt_slot(cur, bsi);
+  const float g = ns->g;
+  const float *ring = a.ring + nd.ring_off;
+
+  // ---- step t: predictor (every lane of the row; the first one writes) ----
+  float th = 0.0f, eps = 0.0f, thh = 0.0f, wh = 0.0f;
+  int deg = 0;
+  if (live) {
+    th = a.theta[gi];
+    const float thh0 = a.theta_hat[gi];
+    const float wh0 = a.omega_hat[gi];
+    float diff = th - thh0;
+    diff = wrap_pm_pi(diff);
+    eps = sinf(diff);
+    thh = thh0 + dt * wh0;
+    wh = wh0 + nd.kappa_w * dt * eps;
+    const int *rp = a.row_ptr + nd.rp_off + row;
+    deg = rp[1] - rp[0];
+  }
+
+  const int slice_row0 = row0 + 32 * (warp >> 2);
+  const bool slice_live = slice_row0 < N;  // warp-uniform
+  int len = 0;
+  const uint32_t *cdp = nullptr;
+  float *wp = nullptr, *wo = nullptr;
+  if (slice_live) {
+    const long long s = nd.slice_base + (slice_row0 >> 5);
+    len = a.sl_len[s];
+    const long long base = a.sl_off[s] + (rloc & 31);
+    cdp = a.sl_cd + base;
+    wp = a.sl_w + base;
+    wo = (a.w2 ? a.w2 : a.sl_w) + base;
+  }
+
+  // ---- step t: edges ------------------------------------------------------
+  float sum0 = 0.0f;
+  if (slice_live)
+    sum0 = row_walk4<MATH, U, 0>(cdp, wp, wp, len, deg, ring, cur, bsi, Np, th, fabsf(eps),
+                                 dt, nd, q, lead);
+  sum0 = __shfl_sync(mask, sum0, lead);
+
+  // ---- step t: integrate; step t+1: predictor ------------------------------
+  float my_cos = 0.0f, my_sin = 0.0f;
+  float th1 = 0.0f, eps1 = 0.0f;
+  if (live) {
+    float inc = dt * (a.omega[gi] + g * sum0 - nd.alpha * eps);
+    float x = th + inc;
+    x = wrap_0_2pi(x);
+    if (!isfinite(x)) x = 0.0f;
+    th1 = x;
+    float diff = th1 - thh;
+    diff = wrap_pm_pi(diff);
+    eps1 = sinf(diff);
+    if (q == 0) {
+      a.theta[gi] = x;
+      a.ring[nd.ring_off + (long long)nxt * Np + row] = x;
+      lev_sincos<MATH>(x, &my_sin, &my_cos);
+      if (a.thh2) {  // speculative: the state stays that after step t
+        a.theta_hat[gi] = thh;
+        a.omega_hat[gi] = wh;
+        a.thh2[gi] = thh + dt * wh;
+        a.omh2[gi] = wh + nd.kappa_w * dt * eps1;
+      } else {
+        a.theta_hat[gi] = thh + dt * wh;
+        a.omega_hat[gi] = wh + nd.kappa_w * dt * eps1;
+      }
+    }
+  }
+
+  // ---- step t+1: edges; the integrate waits for g(t+1) (finish_kernel) ------
+  float sum1 = 0.0f;
+  if (slice_live)
+    sum1 = row_walk4<MATH, U, 1>(cdp, wp, wo, len, deg, ring, nxt, bsi, Np, th1, fabsf(eps1),
+                                 dt, nd, q, lead);
+  if (live && q == 0) a.pend[gi] = make_float2(sum1, eps1);
+
+  // ---- partial of r(t+1): the rows' values in row order, then the tree ----
+  if (q == 0) {
+    s_oc[rloc] = my_cos;
+    s_os[rloc] = my_sin;
+  }
+  __syncthreads();
+  const float c = (tid < kTile) ? s_oc[tid] : 0.0f;
+  const float sv = (tid < kTile) ? s_os[tid] : 0.0f;
+  tile_partial(a, nd, row0, c, sv, s_rc, s_rs);
+}
+
 // The integrate of step t+1 (integrate_and_reduce_kernel, :182-196) with
 // g(t+1), from the coupling sum and eps that pair_kernel parked, and the tile
 // partials of r(t+2).  A CTA takes kFinishTiles consecutive tiles of the

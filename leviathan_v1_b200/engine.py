@@ -45,9 +45,10 @@ def variant_info(v: int) -> dict:
 def pair_variant_info(v: int) -> dict:
     """Tuning parameters of compiled two-steps-per-launch variant ``v``."""
     lib = _lib.load()
-    u, m, dp = C.c_int32(), C.c_int32(), C.c_int32()
+    u, m, dp, ln = C.c_int32(), C.c_int32(), C.c_int32(), C.c_int32()
     check(lib.lev_pair_variant_info(int(v), C.byref(u), C.byref(m), C.byref(dp)))
-    return dict(unroll=u.value, min_blocks=m.value, deep=dp.value)
+    check(lib.lev_pair_variant_lanes(int(v), C.byref(ln)))
+    return dict(unroll=u.value, min_blocks=m.value, deep=dp.value, lanes_per_row=ln.value)
 
 
 class _EngineBase:
@@ -308,9 +309,10 @@ class _EngineBase:
 
     def create_profile(self) -> dict:
         """Milliseconds of the phases of this engine's creation."""
-        ms = (C.c_double * 6)()
+        ms = (C.c_double * 8)()
         check(self._lib.lev_create_profile(self.handle, ms))
-        keys = ("layout", "resources", "node_uploads", "edge_uploads", "convert", "fill")
+        keys = ("layout", "stream_and_kernel_setup", "device_allocation", "mapped_host_buffer",
+                "small_uploads", "staged_uploads", "fill_launch", "dma_wait")
         return {k: float(v) for k, v in zip(keys, ms)}
 
     def set_grid_wait(self, limit_ns: int = 2_000_000_000, extra_arrivals: int = 0) -> None:
