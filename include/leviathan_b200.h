@@ -118,8 +118,12 @@ int lev_batch_create(LevEngine **out, int32_t num_nets, const int32_t *N,
                      const float *theta_hat_cat, const float *omega_cat,
                      const LevParams *params, int32_t math_mode);
 
-/* Replaces leviathan_free (leviathan_kernel.cu:455-478). */
+/* Replaces leviathan_free (leviathan_kernel.cu:455-478).  The engine's
+ * device memory goes back to this library's per-device memory pool, which
+ * keeps it for the next engine created in the process (no driver
+ * allocation then); lev_trim_memory returns the pooled memory to the device. */
 int lev_destroy(LevEngine *h);
+int lev_trim_memory(void);
 
 /* Wall-clock milliseconds of the phases of the engine's creation (no
  * reference counterpart; for tuning construction): ms_out[8] = host-side
@@ -294,8 +298,10 @@ int lev_set_grid_wait(LevEngine *h, uint64_t limit_ns, uint32_t extra_arrivals);
  * (lev_step_n / lev_step_n_async) walk each row's edges for steps t and t+1
  * in one launch and finish step t+1's integrate, which needs the gain
  * g(t+1) and so the global r(t+1), in a short node-only launch.  The
- * edge streams then leave HBM once per two steps.  `deep` variants keep two
- * groups of edges in flight per lane.
+ * edge streams then leave HBM once per two steps.  `deep` 1 variants keep two
+ * groups of edges in flight per lane; `deep` 2 variants copy each warp's SELL
+ * slice into shared memory (cp.async) and walk it there twice, the first
+ * walk's weights staying on chip.
  * Results are bitwise those of one step per launch.  lev_autotune times the pair variants of each
  * degree class against its best one-step variant and keeps pairs only where
  * they are faster; pair_variant -1 means one step per launch for that class.

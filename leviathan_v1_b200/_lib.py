@@ -69,6 +69,7 @@ PROTOTYPES = {
                                    _P, _P, _P, C.POINTER(LevParams), _i32]),
     "lev_destroy": (C.c_int, [_P]),
     "lev_create_profile": (C.c_int, [_P, _P]),
+    "lev_trim_memory": (C.c_int, []),
     "lev_num_nets": (C.c_int, [_P, C.POINTER(_i32)]),
     "lev_total_nodes": (C.c_int, [_P, C.POINTER(_i64)]),
     "lev_total_edges": (C.c_int, [_P, C.POINTER(_i64)]),

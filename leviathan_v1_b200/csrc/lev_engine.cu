@@ -88,21 +88,28 @@ constexpr int kNumVariants = sizeof(kVariants) / sizeof(kVariants[0]);
 // walks); more CTAs win at the small networks of a sweep.
 // LANES: threads per row (1: pair_kernel, 256-thread CTAs; 4: pair4_kernel,
 // 1024-thread CTAs for low-degree rows).
+// SMEM: dynamic shared memory per CTA (pair_smem_kernel: the warps' staged
+// slices; DEEP = 2 marks these variants).
 struct PairVariant {
-  int U, MINB, DEEP, LANES;
+  int U, MINB, DEEP, LANES, SMEM;
   StepFn fn[2];  // [math mode]
 };
 #define LEV_PAIR_VARIANT(U, M, D) \
-  { U, M, D, 1, { pair_kernel<0, U, M, D>, pair_kernel<1, U, M, D> } }
+  { U, M, D, 1, 0, { pair_kernel<0, U, M, D>, pair_kernel<1, U, M, D> } }
 #define LEV_PAIR4_VARIANT(U, M) \
-  { U, M, 0, 4, { pair4_kernel<0, U, M>, pair4_kernel<1, U, M> } }
+  { U, M, 0, 4, 0, { pair4_kernel<0, U, M>, pair4_kernel<1, U, M> } }
+#define LEV_PAIRS_VARIANT(U, M, L)                  \
+  { U, M, 2, 1, pair_smem_bytes<L>(),               \
+    { pair_smem_kernel<0, U, M, L>, pair_smem_kernel<1, U, M, L> } }
 static const PairVariant kPairVariants[] = {
     LEV_PAIR_VARIANT(8, 2, 1), LEV_PAIR_VARIANT(6, 3, 1), LEV_PAIR_VARIANT(8, 3, 0),
     LEV_PAIR_VARIANT(4, 4, 1), LEV_PAIR_VARIANT(10, 2, 1), LEV_PAIR4_VARIANT(2, 1),
-    LEV_PAIR4_VARIANT(4, 1),
+    LEV_PAIR4_VARIANT(4, 1), LEV_PAIRS_VARIANT(8, 2, 48), LEV_PAIRS_VARIANT(12, 2, 48),
+    LEV_PAIRS_VARIANT(6, 3, 32),
 };
 #undef LEV_PAIR_VARIANT
 #undef LEV_PAIR4_VARIANT
+#undef LEV_PAIRS_VARIANT
 constexpr int kNumPairVariants = sizeof(kPairVariants) / sizeof(kPairVariants[0]);
 
 // Networks of a batch are grouped by the mean SELL slice length (the
@@ -280,6 +287,84 @@ int dev_alloc(LevEngine *h, T **p, size_t count) {
   return LEV_OK;
 }
 
+// Device memory of engines comes from one stream-ordered pool per device
+// that keeps freed memory for the next engine of the process (creating an
+// engine then costs no driver allocation when an earlier one was freed);
+// lev_trim_memory gives it back to the device.
+constexpr int kMaxDevices = 64;
+std::mutex g_pool_mu;
+cudaMemPool_t g_pool[kMaxDevices] = {};
+
+cudaError_t engine_pool(int dev, cudaMemPool_t *out) {
+  if (dev < 0 || dev >= kMaxDevices) return cudaErrorInvalidDevice;
+  std::lock_guard<std::mutex> lk(g_pool_mu);
+  if (!g_pool[dev]) {
+    cudaMemPoolProps props = {};
+    props.allocType = cudaMemAllocationTypePinned;
+    props.location.type = cudaMemLocationTypeDevice;
+    props.location.id = dev;
+    cudaError_t e = cudaMemPoolCreate(&g_pool[dev], &props);
+    if (e != cudaSuccess) {
+      g_pool[dev] = nullptr;
+      return e;
+    }
+    uint64_t keep = ~0ull;
+    e = cudaMemPoolSetAttribute(g_pool[dev], cudaMemPoolAttrReleaseThreshold, &keep);
+    if (e != cudaSuccess) return e;
+  }
+  *out = g_pool[dev];
+  return cudaSuccess;
+}
+
+// The r of the last single step is written by the kernel into mapped host
+// memory.  Engines take 4 KiB slots of one mapped block per process (a
+// mapped allocation of its own costs milliseconds); an engine with more
+// networks than a slot holds gets its own.
+constexpr size_t kMapSlot = 4096;
+constexpr int kMapSlots = 256;
+struct MappedArena {
+  std::mutex mu;
+  char *base = nullptr;
+  bool used[kMapSlots] = {};
+};
+MappedArena g_map;
+
+float *mapped_alloc(size_t n_floats) {
+  if (n_floats * sizeof(float) <= kMapSlot) {
+    std::lock_guard<std::mutex> lk(g_map.mu);
+    if (!g_map.base &&
+        cudaHostAlloc(reinterpret_cast<void **>(&g_map.base), kMapSlot * kMapSlots,
+                      cudaHostAllocMapped | cudaHostAllocPortable) != cudaSuccess) {
+      cudaGetLastError();
+      g_map.base = nullptr;
+    }
+    if (g_map.base)
+      for (int k = 0; k < kMapSlots; ++k)
+        if (!g_map.used[k]) {
+          g_map.used[k] = true;
+          return reinterpret_cast<float *>(g_map.base + k * kMapSlot);
+        }
+  }
+  float *p = nullptr;
+  if (cudaHostAlloc(reinterpret_cast<void **>(&p), std::max<size_t>(n_floats, 1) * sizeof(float),
+                    cudaHostAllocMapped | cudaHostAllocPortable) != cudaSuccess)
+    return nullptr;
+  return p;
+}
+
+void mapped_free(float *p) {
+  if (!p) return;
+  {
+    std::lock_guard<std::mutex> lk(g_map.mu);
+    char *c = reinterpret_cast<char *>(p);
+    if (g_map.base && c >= g_map.base && c < g_map.base + kMapSlot * kMapSlots) {
+      g_map.used[(c - g_map.base) / kMapSlot] = false;
+      return;
+    }
+  }
+  cudaFreeHost(p);
+}
+
 void free_engine(LevEngine *h) {
   if (!h) return;
   if (h->hubs) h->hubs->engine = nullptr;
@@ -318,9 +403,9 @@ void free_engine(LevEngine *h) {
   dfree(h->d_rhist);
   dfree(h->d_gwsum);
   dfree(h->d_gbar);
-  if (h->slab) cudaFree(h->slab);
+  if (h->slab) cudaFreeAsync(h->slab, h->stream);  // back to the engine pool
   if (h->h_gerr) cudaFreeHost(h->h_gerr);
-  if (h->h_rmap) cudaFreeHost(h->h_rmap);
+  mapped_free(h->h_rmap);
   if (h->h_rstage) cudaFreeHost(h->h_rstage);
   for (int c = 0; c < kNumClasses; ++c) {
     if (h->class_stream[c]) cudaStreamDestroy(h->class_stream[c]);
@@ -429,11 +514,20 @@ int prepare_step_kernels() {
           cudaFuncAttributePreferredSharedMemoryCarveout,
           (int)cudaSharedmemCarveoutMaxL1));
   for (int v = 0; v < kNumPairVariants; ++v)
-    for (int m = 0; m < 2; ++m)
-      LEV_TRY_CUDA(cudaFuncSetAttribute(
-          reinterpret_cast<const void *>(kPairVariants[v].fn[m]),
-          cudaFuncAttributePreferredSharedMemoryCarveout,
-          (int)cudaSharedmemCarveoutMaxL1));
+    for (int m = 0; m < 2; ++m) {
+      const void *fn = reinterpret_cast<const void *>(kPairVariants[v].fn[m]);
+      const int smem = kPairVariants[v].SMEM;
+      if (smem > 0) {
+        // staged slices: room for MINB CTAs' slices, the rest stays L1
+        LEV_TRY_CUDA(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+        const int pct = std::min(100, (kPairVariants[v].MINB * (smem + 1024) * 100 +
+                                       (228 << 10) - 1) / (228 << 10));
+        LEV_TRY_CUDA(cudaFuncSetAttribute(fn, cudaFuncAttributePreferredSharedMemoryCarveout, pct));
+      } else {
+        LEV_TRY_CUDA(cudaFuncSetAttribute(fn, cudaFuncAttributePreferredSharedMemoryCarveout,
+                                          (int)cudaSharedmemCarveoutMaxL1));
+      }
+    }
   return LEV_OK;
 }
 
@@ -490,8 +584,9 @@ int launch_pair_class(LevEngine *h, int c, StepArgs a, int phase, cudaStream_t s
             ? reinterpret_cast<const void *>(kVariants[tc.variant].fn[mode])
             : reinterpret_cast<const void *>(kPairVariants[tc.pair_variant].fn[mode]);
     const int lanes = tc.pair_variant < 0 ? 1 : kPairVariants[tc.pair_variant].LANES;
+    const int smem = tc.pair_variant < 0 ? 0 : kPairVariants[tc.pair_variant].SMEM;
     void *args[] = {&a};
-    LEV_TRY_CUDA(cudaLaunchKernel(fn, dim3(tc.ntiles), dim3(lanes * kTile), args, 0, s));
+    LEV_TRY_CUDA(cudaLaunchKernel(fn, dim3(tc.ntiles), dim3(lanes * kTile), args, smem, s));
   } else {
     const int blocks = (tc.ntiles + kFinishTiles - 1) / kFinishTiles;
     if (mode)
@@ -1431,10 +1526,13 @@ int create_impl(LevEngine **out, int num_nets, const int32_t *Ns,
     size_t total = 0;
     for (const Part &q : parts) total += (q.bytes + 255) / 256 * 256;
     if (rc == LEV_OK) {
-      cudaError_t e = cudaMalloc(&h->slab, total);
+      cudaMemPool_t pool = nullptr;
+      cudaError_t e = engine_pool(h->device, &pool);
+      if (e == cudaSuccess) e = cudaMallocFromPoolAsync(&h->slab, total, pool, h->stream);
       if (e != cudaSuccess) {
+        cudaGetLastError();
         h->slab = nullptr;
-        rc = fail(LEV_ERR_NOMEM, std::string("cudaMalloc of ") + std::to_string(total) +
+        rc = fail(LEV_ERR_NOMEM, std::string("device allocation of ") + std::to_string(total) +
                                      " bytes failed: " + cudaGetErrorString(e));
       }
     }
@@ -1454,8 +1552,8 @@ int create_impl(LevEngine **out, int num_nets, const int32_t *Ns,
     return fail(rc, msg);
   }
   mark(2);
-  ce = cudaHostAlloc(reinterpret_cast<void **>(&h->h_rmap),
-                     sizeof(float) * num_nets, cudaHostAllocMapped);
+  h->h_rmap = mapped_alloc((size_t)num_nets);
+  ce = h->h_rmap ? cudaSuccess : cudaErrorMemoryAllocation;
   if (ce == cudaSuccess)
     ce = cudaHostGetDevicePointer(reinterpret_cast<void **>(&h->d_rmap),
                                   h->h_rmap, 0);
@@ -2142,6 +2240,13 @@ int lev_set_grid_wait(LevEngine *h, uint64_t limit_ns, uint32_t extra_arrivals) 
   if (rc != LEV_OK) return rc;
   h->grid_wait.ns = limit_ns;
   h->grid_wait.extra = extra_arrivals;
+  return LEV_OK;
+}
+
+int lev_trim_memory(void) {
+  std::lock_guard<std::mutex> lk(g_pool_mu);
+  for (int d = 0; d < kMaxDevices; ++d)
+    if (g_pool[d]) LEV_TRY_CUDA(cudaMemPoolTrimTo(g_pool[d], 0));
   return LEV_OK;
 }
 
