@@ -396,6 +396,7 @@ def run_batched(args, rank, world, plain_value):
     N_local = sum(n.N for n in nets)
     eng = BatchEngine([n.as_dict() for n in nets], params=params)
     tune = eng.autotune(DT, trial_steps=5)  # the state is restored afterwards
+    pair_info = eng.pair_info()
     # FP64 error over a 10-step prefix of four sampled networks (K spread),
     # from the initial state; the timing below continues from there
     picks = [i for i in np.argsort([p["g"] for p in params])[[0, len(nets) // 3,
@@ -448,7 +449,7 @@ def run_batched(args, rank, world, plain_value):
             "serial_engines_note": "16 sampled networks, one engine each, 50 steps "
                                    "per call incl. engine construction",
             "autotune": {"chosen": tune["chosen"], "ms": tune["ms"],
-                         "variants": tune["variants"]},
+                         "variants": tune["variants"], "pairs": pair_info},
             "r_of_K_bins_0_to_4": r_of_K,
             "fp64_error_prefix": fp64,
             "algorithmic_bytes_per_step": int(17 * E_tot + 36 * N_tot)}

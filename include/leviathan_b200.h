@@ -298,10 +298,8 @@ int lev_set_grid_wait(LevEngine *h, uint64_t limit_ns, uint32_t extra_arrivals);
  * (lev_step_n / lev_step_n_async) walk each row's edges for steps t and t+1
  * in one launch and finish step t+1's integrate, which needs the gain
  * g(t+1) and so the global r(t+1), in a short node-only launch.  The
- * edge streams then leave HBM once per two steps.  `deep` 1 variants keep two
- * groups of edges in flight per lane; `deep` 2 variants copy each warp's SELL
- * slice into shared memory (cp.async) and walk it there twice, the first
- * walk's weights staying on chip.
+ * edge streams then leave HBM once per two steps.  `deep` variants keep two
+ * groups of edges in flight per lane.
  * Results are bitwise those of one step per launch.  lev_autotune times the pair variants of each
  * degree class against its best one-step variant and keeps pairs only where
  * they are faster; pair_variant -1 means one step per launch for that class.

@@ -88,28 +88,21 @@ constexpr int kNumVariants = sizeof(kVariants) / sizeof(kVariants[0]);
 // walks); more CTAs win at the small networks of a sweep.
 // LANES: threads per row (1: pair_kernel, 256-thread CTAs; 4: pair4_kernel,
 // 1024-thread CTAs for low-degree rows).
-// SMEM: dynamic shared memory per CTA (pair_smem_kernel: the warps' staged
-// slices; DEEP = 2 marks these variants).
 struct PairVariant {
-  int U, MINB, DEEP, LANES, SMEM;
+  int U, MINB, DEEP, LANES;
   StepFn fn[2];  // [math mode]
 };
 #define LEV_PAIR_VARIANT(U, M, D) \
-  { U, M, D, 1, 0, { pair_kernel<0, U, M, D>, pair_kernel<1, U, M, D> } }
+  { U, M, D, 1, { pair_kernel<0, U, M, D>, pair_kernel<1, U, M, D> } }
 #define LEV_PAIR4_VARIANT(U, M) \
-  { U, M, 0, 4, 0, { pair4_kernel<0, U, M>, pair4_kernel<1, U, M> } }
-#define LEV_PAIRS_VARIANT(U, M, L)                  \
-  { U, M, 2, 1, pair_smem_bytes<L>(),               \
-    { pair_smem_kernel<0, U, M, L>, pair_smem_kernel<1, U, M, L> } }
+  { U, M, 0, 4, { pair4_kernel<0, U, M>, pair4_kernel<1, U, M> } }
 static const PairVariant kPairVariants[] = {
     LEV_PAIR_VARIANT(8, 2, 1), LEV_PAIR_VARIANT(6, 3, 1), LEV_PAIR_VARIANT(8, 3, 0),
     LEV_PAIR_VARIANT(4, 4, 1), LEV_PAIR_VARIANT(10, 2, 1), LEV_PAIR4_VARIANT(2, 1),
-    LEV_PAIR4_VARIANT(4, 1), LEV_PAIRS_VARIANT(8, 2, 48), LEV_PAIRS_VARIANT(12, 2, 48),
-    LEV_PAIRS_VARIANT(6, 3, 32),
+    LEV_PAIR4_VARIANT(4, 1),
 };
 #undef LEV_PAIR_VARIANT
 #undef LEV_PAIR4_VARIANT
-#undef LEV_PAIRS_VARIANT
 constexpr int kNumPairVariants = sizeof(kPairVariants) / sizeof(kPairVariants[0]);
 
 // Networks of a batch are grouped by the mean SELL slice length (the
@@ -514,20 +507,11 @@ int prepare_step_kernels() {
           cudaFuncAttributePreferredSharedMemoryCarveout,
           (int)cudaSharedmemCarveoutMaxL1));
   for (int v = 0; v < kNumPairVariants; ++v)
-    for (int m = 0; m < 2; ++m) {
-      const void *fn = reinterpret_cast<const void *>(kPairVariants[v].fn[m]);
-      const int smem = kPairVariants[v].SMEM;
-      if (smem > 0) {
-        // staged slices: room for MINB CTAs' slices, the rest stays L1
-        LEV_TRY_CUDA(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
-        const int pct = std::min(100, (kPairVariants[v].MINB * (smem + 1024) * 100 +
-                                       (228 << 10) - 1) / (228 << 10));
-        LEV_TRY_CUDA(cudaFuncSetAttribute(fn, cudaFuncAttributePreferredSharedMemoryCarveout, pct));
-      } else {
-        LEV_TRY_CUDA(cudaFuncSetAttribute(fn, cudaFuncAttributePreferredSharedMemoryCarveout,
-                                          (int)cudaSharedmemCarveoutMaxL1));
-      }
-    }
+    for (int m = 0; m < 2; ++m)
+      LEV_TRY_CUDA(cudaFuncSetAttribute(
+          reinterpret_cast<const void *>(kPairVariants[v].fn[m]),
+          cudaFuncAttributePreferredSharedMemoryCarveout,
+          (int)cudaSharedmemCarveoutMaxL1));
   return LEV_OK;
 }
 
@@ -584,9 +568,8 @@ int launch_pair_class(LevEngine *h, int c, StepArgs a, int phase, cudaStream_t s
             ? reinterpret_cast<const void *>(kVariants[tc.variant].fn[mode])
             : reinterpret_cast<const void *>(kPairVariants[tc.pair_variant].fn[mode]);
     const int lanes = tc.pair_variant < 0 ? 1 : kPairVariants[tc.pair_variant].LANES;
-    const int smem = tc.pair_variant < 0 ? 0 : kPairVariants[tc.pair_variant].SMEM;
     void *args[] = {&a};
-    LEV_TRY_CUDA(cudaLaunchKernel(fn, dim3(tc.ntiles), dim3(lanes * kTile), args, smem, s));
+    LEV_TRY_CUDA(cudaLaunchKernel(fn, dim3(tc.ntiles), dim3(lanes * kTile), args, 0, s));
   } else {
     const int blocks = (tc.ntiles + kFinishTiles - 1) / kFinishTiles;
     if (mode)

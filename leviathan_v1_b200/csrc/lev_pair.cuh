@@ -358,205 +358,6 @@ __global__ void __launch_bounds__(kTile, MINB) pair_kernel(const StepArgs a) {
 }
 
 // ---------------------------------------------------------------------------
-// Staged slices: each warp copies its SELL slice (col/delay words and
-// weights, contiguous in HBM) into shared memory once, with cp.async (L2
-// only, so the L1 keeps the ring lines), and both walks read it from there.
-// The first walk's new weights stay in shared memory for the second walk,
-// which writes the final weights to HBM: the edge streams cross L2 once per
-// two steps, and a gather waits only on a shared-memory read of its
-// col/delay word, not on a global load.  Slices longer than LMAX entries per
-// row take the global walk (row_walk).  Same arithmetic and order as
-// row_walk, so results are bitwise those of pair_kernel.
-// ---------------------------------------------------------------------------
-__device__ __forceinline__ void pair_cp16(void *dst, const void *src) {
-  const unsigned d = (unsigned)__cvta_generic_to_shared(dst);
-  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(d), "l"(src) : "memory");
-}
-
-// One walk over a staged slice.  SECOND = 0: new weights into s_w (and, for
-// a speculative pair, also to HBM at wg, the engine state after step t);
-// SECOND = 1: final weights to HBM at wg.  Two stages: the gathers of group
-// k0+U are in flight while group k0 computes.
-template <int MATH, int U, int SECOND>
-__device__ __forceinline__ float row_walk_smem(const uint32_t *s_cd, float *s_w, float *wg,
-                                               bool wg_first, int len, int deg,
-                                               const float *__restrict__ ring, int base,
-                                               int bsi, int Np, float th, float my_eps, float dt,
-                                               const NetDesc &nd, int lane) {
-  const float eta = nd.eta, gamma = nd.gamma, lam = nd.lam;
-  const float w_min = nd.w_min, w_max = nd.w_max;
-  float local_sum = 0.0f;
-  auto gather = [&](int k0, float *g) {
-#pragma unroll
-    for (int u = 0; u < U; ++u) {
-      const int k = k0 + u;
-      g[u] = 0.0f;
-      if (k < deg) {
-        const uint32_t p = s_cd[32 * k + lane];
-        int slot = base - (int)(p & 255u);
-        slot += (slot < 0) ? bsi : 0;
-        g[u] = ld_ring(ring + ((unsigned)slot * (unsigned)Np + (p >> 8)));
-      }
-    }
-  };
-  float ga[U], gb[U];
-  gather(0, ga);
-  for (int k0 = 0; k0 < len; k0 += U) {
-    gather(k0 + U, gb);
-#pragma unroll
-    for (int u = 0; u < U; ++u) {
-      const int k = k0 + u;
-      if (k < deg) {
-        const float delayed_j = ga[u];
-        float diff = delayed_j - th;
-        diff = wrap_pm_pi(diff);
-        float w = s_w[32 * k + lane];
-        float sin_diff, cos_diff;
-        lev_sincos<MATH>(diff, &sin_diff, &cos_diff);
-        local_sum += w * sin_diff;
-        float dw = dt * (eta * cos_diff * (1.0f - gamma * my_eps) - lam * w);
-        w += dw;
-        if (!isfinite(w)) w = w_min;
-        w = fmaxf(w_min, fminf(w_max, w));
-        if (SECOND) {
-          __stcs(wg + 32 * k, w);
-        } else {
-          s_w[32 * k + lane] = w;
-          if (wg_first) __stcg(wg + 32 * k, w);
-        }
-      }
-    }
-#pragma unroll
-    for (int u = 0; u < U; ++u) ga[u] = gb[u];
-  }
-  return local_sum;
-}
-
-template <int LMAX>
-constexpr int pair_smem_bytes() {
-  return (kTile / 32) * 32 * LMAX * 8;  // per warp: col/delay words and weights
-}
-
-template <int MATH, int U, int MINB, int LMAX>
-__global__ void __launch_bounds__(kTile, MINB) pair_smem_kernel(const StepArgs a) {
-  __shared__ float s_rc[32];
-  __shared__ float s_rs[32];
-  extern __shared__ __align__(16) unsigned char s_dyn[];
-
-  const int tid = threadIdx.x;
-  const int lane = tid & 31, warp = tid >> 5;
-  const int tix = a.reverse ? (int)(gridDim.x - 1 - blockIdx.x) : (int)blockIdx.x;
-  const int2 tile = a.tiles[tix];
-  const NetDesc nd = a.nets[tile.x];
-  NetState *ns = a.st + tile.x;
-
-  const int N = nd.N;
-  const int row0 = tile.y;
-  const int row = row0 + tid;
-  const bool live = row < N;
-  const long long gi = nd.node_off + row;
-  const float dt = a.dt;
-  const int bsi = nd.bsi;
-  const int Np = nd.Np;
-  const int cur = ns->cur;
-  const int nxt = nxt_slot(cur, bsi);
-  const float g = ns->g;
-  const float *ring = a.ring + nd.ring_off;
-  uint32_t *s_cd = reinterpret_cast<uint32_t *>(s_dyn) + warp * (64 * LMAX);
-  float *s_w = reinterpret_cast<float *>(s_cd + 32 * LMAX);
-
-  const int slice_row0 = row0 + 32 * warp;
-  const bool slice_live = slice_row0 < N;  // warp-uniform
-  int len = 0;
-  long long base = 0;
-  if (slice_live) {
-    const long long s = nd.slice_base + (slice_row0 >> 5);
-    len = a.sl_len[s];
-    base = a.sl_off[s];
-    if (len <= LMAX) {  // stage the slice: 8 * len 16-byte pieces per stream
-      const uint32_t *cd = a.sl_cd + base;
-      const float *w = a.sl_w + base;
-      for (int c = lane; c < 8 * len; c += 32) {
-        pair_cp16(s_cd + 4 * c, cd + 4 * c);
-        pair_cp16(s_w + 4 * c, w + 4 * c);
-      }
-      asm volatile("cp.async.commit_group;" ::: "memory");
-    }
-  }
-
-  // ---- step t: predictor (while the slice arrives) --------------------------
-  float th = 0.0f, eps = 0.0f, thh = 0.0f, wh = 0.0f;
-  int deg = 0;
-  if (live) {
-    th = a.theta[gi];
-    const float thh0 = a.theta_hat[gi];
-    const float wh0 = a.omega_hat[gi];
-    float diff = th - thh0;
-    diff = wrap_pm_pi(diff);
-    eps = sinf(diff);
-    thh = thh0 + dt * wh0;
-    wh = wh0 + nd.kappa_w * dt * eps;
-    const int *rp = a.row_ptr + nd.rp_off + row;
-    deg = rp[1] - rp[0];
-  }
-  const bool staged = slice_live && len <= LMAX;
-  if (staged) {
-    asm volatile("cp.async.wait_all;" ::: "memory");
-    __syncwarp();
-  }
-  const uint32_t *cdp = a.sl_cd + base + lane;
-  float *wp = a.sl_w + base + lane;
-  float *wo = (a.w2 ? a.w2 : a.sl_w) + base + lane;
-
-  // ---- step t: edges --------------------------------------------------------
-  float sum0 = 0.0f;
-  if (staged)
-    sum0 = row_walk_smem<MATH, U, 0>(s_cd, s_w, wp, a.w2 != nullptr, len, deg, ring, cur, bsi,
-                                     Np, th, fabsf(eps), dt, nd, lane);
-  else if (slice_live)
-    sum0 = row_walk<MATH, U, 0, 1>(cdp, wp, wp, len, deg, ring, cur, bsi, Np, th, fabsf(eps),
-                                   dt, nd);
-
-  // ---- step t: integrate; step t+1: predictor ------------------------------
-  float my_cos = 0.0f, my_sin = 0.0f;
-  float th1 = 0.0f, eps1 = 0.0f;
-  if (live) {
-    float inc = dt * (a.omega[gi] + g * sum0 - nd.alpha * eps);
-    float x = th + inc;
-    x = wrap_0_2pi(x);
-    if (!isfinite(x)) x = 0.0f;
-    th1 = x;
-    a.theta[gi] = x;
-    a.ring[nd.ring_off + (long long)nxt * Np + row] = x;
-    lev_sincos<MATH>(x, &my_sin, &my_cos);
-    float diff = th1 - thh;
-    diff = wrap_pm_pi(diff);
-    eps1 = sinf(diff);
-    if (a.thh2) {  // speculative: the state stays that after step t
-      a.theta_hat[gi] = thh;
-      a.omega_hat[gi] = wh;
-      a.thh2[gi] = thh + dt * wh;
-      a.omh2[gi] = wh + nd.kappa_w * dt * eps1;
-    } else {
-      a.theta_hat[gi] = thh + dt * wh;
-      a.omega_hat[gi] = wh + nd.kappa_w * dt * eps1;
-    }
-  }
-
-  // ---- step t+1: edges --------------------------------------------------------
-  float sum1 = 0.0f;
-  if (staged)
-    sum1 = row_walk_smem<MATH, U, 1>(s_cd, s_w, wo, false, len, deg, ring, nxt, bsi, Np, th1,
-                                     fabsf(eps1), dt, nd, lane);
-  else if (slice_live)
-    sum1 = row_walk<MATH, U, 1, 1>(cdp, wp, wo, len, deg, ring, nxt, bsi, Np, th1, fabsf(eps1),
-                                   dt, nd);
-  if (live) a.pend[gi] = make_float2(sum1, eps1);
-
-  tile_partial(a, nd, row0, my_cos, my_sin, s_rc, s_rs);
-}
-
-// ---------------------------------------------------------------------------
 // Four lanes per row: the threads-per-row dimension of the autotuner.  A row
 // of a low-degree network is only a few SELL entries long, so one lane per
 // row leaves most of the gathers' latency exposed; four lanes per row keep
