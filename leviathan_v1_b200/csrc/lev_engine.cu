@@ -1044,17 +1044,18 @@ struct StageJob {
 // bit 1 a column out of range, bit 2 a delay above max_delay, bit 4 a zero
 // delay.  Padding entries are node 0, delay 0, weight 0 (read, never used).
 unsigned pack_slices(const PackSrc &ps, long long s0, long long s1, int k0, int k1,
-                     uint32_t *cd, float *w) {
+                     uint32_t *__restrict__ cd, float *__restrict__ w) {
   unsigned bad = 0u;
   size_t o = 0;
   for (long long s = s0; s < s1; ++s) {
     const int n = (*ps.slice_net)[s];
     const NetDesc &d = (*ps.nets)[n];
     const int32_t *rp = ps.rp_cat + d.rp_off;
-    const int32_t *col = ps.col_cat + d.edge_off;
-    const uint8_t *dl = ps.dl_cat + d.edge_off;
-    const float *wv = ps.w_cat + d.edge_off;
+    const int32_t *__restrict__ col = ps.col_cat + d.edge_off;
+    const uint8_t *__restrict__ dl = ps.dl_cat + d.edge_off;
+    const float *__restrict__ wv = ps.w_cat + d.edge_off;
     const int ncols = d.N + (n == 0 ? ps.n_ext : 0);
+    const unsigned md = (unsigned)d.max_delay;
     const int row0 = (int)(s - d.slice_base) * 32;
     const int len = (*ps.sl_len)[s];
     const bool part = (k1 >= 0);
@@ -1070,9 +1071,8 @@ unsigned pack_slices(const PackSrc &ps, long long s0, long long s1, int k0, int 
       for (int k = ka; k < kd; ++k) {
         const int c = col[e0 + k];
         const unsigned de = dl[e0 + k];
-        if (c < 0 || c >= ncols) bad |= 1u;
-        if ((int)de > d.max_delay) bad |= 2u;
-        if (de == 0u) bad |= 4u;
+        bad |= (unsigned)((unsigned)c >= (unsigned)ncols) | ((unsigned)(de > md) << 1) |
+               ((unsigned)(de == 0u) << 2);
         cd[o + 32 * (size_t)(k - ka) + l] = ((uint32_t)c << 8) | de;
         w[o + 32 * (size_t)(k - ka) + l] = wv[e0 + k];
       }
