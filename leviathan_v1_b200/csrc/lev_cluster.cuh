@@ -174,7 +174,7 @@ __global__ void __launch_bounds__(MAXR, 1) cluster_kernel(const ClusterArgs a) {
     deg = rp[1] - rp[0];
   }
   for (int s = 0; s < bsi; ++s)
-    if (live) s_ring[(size_t)s * R + tid] = a.ring[nd.ring_off + (long long)s * Np + row];
+    if (live) s_ring[(size_t)s * R + tid] = a.ring[nd.ring_off + ring_pos(s, row, Np)];
   NetState ns = *a.st;
   int cur = ns.cur, rbuf = ns.rbuf;
   float g = ns.g, r = ns.r;
@@ -329,7 +329,7 @@ __global__ void __launch_bounds__(MAXR, 1) cluster_kernel(const ClusterArgs a) {
     a.theta_hat[gi] = s_thh[tid];
     a.omega_hat[gi] = s_omh[tid];
     for (int s = 0; s < bsi; ++s)
-      a.ring[nd.ring_off + (long long)s * Np + row] = s_ring[(size_t)s * R + tid];
+      a.ring[nd.ring_off + ring_pos(s, row, Np)] = s_ring[(size_t)s * R + tid];
   }
   for (int k = tid; k < nent; k += blockDim.x) a.sl_w[ebase + k] = s_w[k];
   // no CTA may leave while a peer can still read its shared memory
@@ -409,7 +409,7 @@ __global__ void __launch_bounds__(4 * 128, 1) cluster_split_kernel(const Cluster
     deg = rp[1] - rp[0];
   }
   for (int s = q; s < bsi; s += LPR)
-    if (live) s_ring[(size_t)s * R + rloc] = a.ring[nd.ring_off + (long long)s * Np + row];
+    if (live) s_ring[(size_t)s * R + rloc] = a.ring[nd.ring_off + ring_pos(s, row, Np)];
   NetState ns = *a.st;
   int cur = ns.cur, rbuf = ns.rbuf;
   float g = ns.g, r = ns.r;
@@ -584,7 +584,7 @@ __global__ void __launch_bounds__(4 * 128, 1) cluster_split_kernel(const Cluster
       a.omega_hat[gi] = s_omh[rloc];
     }
     for (int s = q; s < bsi; s += LPR)
-      a.ring[nd.ring_off + (long long)s * Np + row] = s_ring[(size_t)s * R + rloc];
+      a.ring[nd.ring_off + ring_pos(s, row, Np)] = s_ring[(size_t)s * R + rloc];
   }
   for (int k = tid; k < nent; k += blockDim.x) a.sl_w[ebase + k] = s_w[k];
   // no CTA may leave while a peer can still read its shared memory

@@ -461,7 +461,7 @@ int launch_fill(LevEngine *h, int n) {
   const long long total = (long long)nd.bsi * nd.N;
   int blocks = (int)std::min<long long>((total + 255) / 256, 148LL * 16);
   ring_fill_kernel<<<blocks, 256, 0, h->stream>>>(
-      h->d_theta + nd.node_off, h->d_ring + nd.ring_off, nd.N, nd.Np, nd.bsi);
+      h->d_theta + nd.node_off, h->d_ring + nd.ring_off, nd.N, nd.Np, nd.bsi, 0, 1);
   LEV_TRY_CUDA(cudaGetLastError());
   return LEV_OK;
 }
@@ -1256,7 +1256,7 @@ int fill_ext_columns(LevEngine *h, int n_ext, const float *theta_ext) {
     const long long total = (long long)nd.bsi * n_ext;
     int blocks = (int)std::min<long long>((total + 255) / 256, 148LL * 16);
     ring_fill_kernel<<<blocks, 256, 0, h->stream>>>(
-        d_tmp, h->d_ring + nd.ring_off + nd.N, n_ext, nd.Np, nd.bsi);
+        d_tmp, h->d_ring + nd.ring_off, n_ext, nd.Np, nd.bsi, nd.N, 1);
     e = cudaGetLastError();
   }
   if (e == cudaSuccess) e = cudaStreamSynchronize(h->stream);
@@ -1365,7 +1365,7 @@ int create_impl(LevEngine **out, int num_nets, const int32_t *Ns,
     }
     params_to_desc(p, &d);
     // ring gathers index a network's ring with 32-bit slot * Np + col
-    if ((unsigned long long)d.bsi * (unsigned long long)d.Np >= (1ull << 32)) {
+    if ((unsigned long long)ring_slots(d.bsi) * (unsigned long long)d.Np >= (1ull << 32)) {
       delete h;
       return fail(LEV_ERR_ARG, "network " + std::to_string(n) +
                                    ": (max_delay + 2) * N must be below 2^32");
@@ -1384,7 +1384,7 @@ int create_impl(LevEngine **out, int num_nets, const int32_t *Ns,
     h->net_E[n] = E;
     node_off += N;
     edge_off += E;
-    ring_off += (long long)d.bsi * d.Np;
+    ring_off += (long long)ring_slots(d.bsi) * d.Np;
     rp_off += N + 1;
     tiles += d.ntiles;
   }
@@ -1997,7 +1997,7 @@ int lev_get_ring(LevEngine *h, int32_t net, float *ring_out,
   int rc = read_states(h, st);
   if (rc != LEV_OK) return rc;
   const NetDesc &d = h->h_nets[net];
-  std::vector<float> ri((size_t)d.bsi * d.Np);
+  std::vector<float> ri((size_t)ring_slots(d.bsi) * d.Np);
   LEV_TRY_CUDA(cudaMemcpyAsync(ri.data(), h->d_ring + d.ring_off,
                                sizeof(float) * ri.size(),
                                cudaMemcpyDeviceToHost, h->stream));
@@ -2007,8 +2007,7 @@ int lev_get_ring(LevEngine *h, int32_t net, float *ring_out,
   for (int m = 0; m <= d.max_delay; ++m) {
     const int si = ((cur - m) % d.bsi + d.bsi) % d.bsi;
     const int sr = ((rb - m) % bs + bs) % bs;
-    const float *src = ri.data() + (size_t)si * d.Np;
-    for (int j = 0; j < d.N; ++j) ring_out[(size_t)j * bs + sr] = src[j];
+    for (int j = 0; j < d.N; ++j) ring_out[(size_t)j * bs + sr] = ri[ring_pos(si, j, d.Np)];
   }
   if (buf_idx) *buf_idx = rb;
   return LEV_OK;
@@ -2028,13 +2027,12 @@ int lev_set_ring(LevEngine *h, int32_t net, const float *ring_in,
   std::vector<NetState> st;
   int rc = read_states(h, st);
   if (rc != LEV_OK) return rc;
-  std::vector<float> ri((size_t)d.bsi * d.Np, 0.0f);
+  std::vector<float> ri((size_t)ring_slots(d.bsi) * d.Np, 0.0f);
   const int cur = st[net].cur;
   for (int m = 0; m <= d.max_delay; ++m) {
     const int si = ((cur - m) % d.bsi + d.bsi) % d.bsi;
     const int sr = ((buf_idx - m) % bs + bs) % bs;
-    float *dst = ri.data() + (size_t)si * d.Np;
-    for (int j = 0; j < d.N; ++j) dst[j] = ring_in[(size_t)j * bs + sr];
+    for (int j = 0; j < d.N; ++j) ri[ring_pos(si, j, d.Np)] = ring_in[(size_t)j * bs + sr];
   }
   LEV_TRY_CUDA(cudaMemcpyAsync(h->d_ring + d.ring_off, ri.data(),
                                sizeof(float) * ri.size(),
@@ -3551,7 +3549,7 @@ int lev_adj_forward(LevAdjoint *a, float dt, int32_t T, const float *omega,
     const long long total = (long long)d.bsi * d.N;
     int fb = (int)std::min<long long>((total + 255) / 256, 148LL * 16);
     ring_fill_kernel<<<fb, 256, 0, s>>>(a->theta0 + d.node_off, a->ring + d.ring_off,
-                                       d.N, d.Np, d.bsi);
+                                       d.N, d.Np, d.bsi, 0, 0);  // slot-major
   }
   adj_state_kernel<<<1, 128, 0, s>>>(0, a->d_nets, a->d_st, nullptr, K, a->NN);
   LEV_TRY_CUDA(cudaGetLastError());

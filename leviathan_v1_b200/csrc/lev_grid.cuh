@@ -267,7 +267,7 @@ __global__ void __launch_bounds__(kGridLPR * R, 256 / R) grid_kernel(const GridA
         for (int u = 0; u < U; ++u) {
           int slot = cur - (int)(p[u] & 255u);
           slot += (slot < 0) ? bsi : 0;
-          dj[u] = __ldcg(ring + (size_t)slot * Np + (int)(p[u] >> 8));
+          dj[u] = __ldcg(ring + ring_pos(slot, p[u] >> 8, Np));
         }
 #pragma unroll
         for (int u = 0; u < U; ++u) {
@@ -332,7 +332,7 @@ __global__ void __launch_bounds__(kGridLPR * R, 256 / R) grid_kernel(const GridA
         x = wrap_0_2pi(x);
         if (!isfinite(x)) x = 0.0f;
         s_th[rloc] = x;
-        __stcg(ring_w + (size_t)nxt * Np + row, x);
+        __stcg(ring_w + ring_pos(nxt, row, Np), x);
         lev_sincos<MATH>(x, &my_sin, &my_cos);
       }
       s_ord[rloc] = my_cos;

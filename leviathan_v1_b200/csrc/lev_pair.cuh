@@ -185,7 +185,7 @@ __device__ __forceinline__ float row_walk(const uint32_t *__restrict__ cdp,
     for (int u = 0; u < U; ++u) {
       int slot = base - (int)(p[u] & 255u);
       slot += (slot < 0) ? bsi : 0;
-      const float *src = ring + ((unsigned)slot * (unsigned)Np + (p[u] >> 8));
+      const float *src = ring + ring_pos(slot, p[u] >> 8, Np);
       if (SECOND)
         g[u] = (k0 + u < deg) ? ld_ring(src) : 0.0f;
       else
@@ -329,7 +329,7 @@ __global__ void __launch_bounds__(kTile, MINB) pair_kernel(const StepArgs a) {
     if (!isfinite(x)) x = 0.0f;
     th1 = x;
     a.theta[gi] = x;
-    a.ring[nd.ring_off + (long long)nxt * Np + row] = x;
+    a.ring[nd.ring_off + ring_pos(nxt, row, Np)] = x;
     lev_sincos<MATH>(x, &my_sin, &my_cos);
     // ---- step t+1: predictor ------------------------------------------------
     float diff = th1 - thh;
@@ -400,7 +400,7 @@ __device__ __forceinline__ float row_walk4(const uint32_t *__restrict__ cdp,
     for (int u = 0; u < U; ++u) {
       int slot = base - (int)(p[u] & 255u);
       slot += (slot < 0) ? bsi : 0;
-      const float *src = ring + ((unsigned)slot * (unsigned)Np + (p[u] >> 8));
+      const float *src = ring + ring_pos(slot, p[u] >> 8, Np);
       dj[u] = (kb + 4 * u + q < deg) ? ld_ring(src) : 0.0f;
     }
 #pragma unroll
@@ -519,7 +519,7 @@ __global__ void __launch_bounds__(4 * kTile, MINB) pair4_kernel(const StepArgs a
     eps1 = sinf(diff);
     if (q == 0) {
       a.theta[gi] = x;
-      a.ring[nd.ring_off + (long long)nxt * Np + row] = x;
+      a.ring[nd.ring_off + ring_pos(nxt, row, Np)] = x;
       lev_sincos<MATH>(x, &my_sin, &my_cos);
       if (a.thh2) {  // speculative: the state stays that after step t
         a.theta_hat[gi] = thh;
@@ -608,7 +608,7 @@ __global__ void __launch_bounds__(kTile) finish_kernel(const StepArgs a, int nti
       x = wrap_0_2pi(x);
       if (!isfinite(x)) x = 0.0f;
       a.theta[gi] = x;
-      a.ring[nd.ring_off + (long long)nxt * nd.Np + row] = x;
+      a.ring[nd.ring_off + ring_pos(nxt, row, nd.Np)] = x;
       if (a.thh2) {  // the predictor of a speculative pair
         a.theta_hat[gi] = a.thh2[gi];
         a.omega_hat[gi] = a.omh2[gi];

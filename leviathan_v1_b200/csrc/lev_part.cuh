@@ -89,11 +89,11 @@ __global__ void part_unpack_kernel(const NetState *st, float *__restrict__ ring,
                                    int N, int Np, int n_halo,
                                    const int *__restrict__ idx, int n,
                                    const float *__restrict__ in) {
-  const long long base = (long long)st->cur * Np + N;
+  const int cur = st->cur;
   for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < n;
        k += gridDim.x * blockDim.x) {
     const int j = idx[k];
-    if ((unsigned)j < (unsigned)n_halo) ring[base + j] = in[k];
+    if ((unsigned)j < (unsigned)n_halo) ring[ring_pos(cur, (unsigned)(N + j), Np)] = in[k];
   }
 }
 
