@@ -19,12 +19,12 @@
 //   sl_cd    uint32[...]        (col_idx << 8) | delay, SELL-32 layout
 //   sl_w     f32   [...]        plastic weights, SELL-32 layout, in place
 //   theta, theta_hat, omega, omega_hat  f32 [N]
-//   ring     f32   [bsi/2][Np][2] delay ring, bsi = max_delay + 2 (rounded up
-//                               to even for the allocation), Np = N rounded up
-//                               to 32: slots 2m and 2m+1 of a node side by side
-//                               (ring_pos), so the two walks of a pair launch
-//                               find slots t-d and t+1-d in one 8-byte word
-//                               for half of the delays
+//   ring     f32   [bsi/4][Np][4] delay ring, bsi = max_delay + 2 (rounded up
+//                               to a multiple of 4 for the allocation), Np = N
+//                               rounded up to 32: slots 4m .. 4m+3 of a node
+//                               side by side (ring_pos), so the two walks of a
+//                               pair launch find slots t-d and t+1-d in one
+//                               16-byte group for three delays in four
 //
 // SELL-32 (sliced ELLPACK, slice height 32): rows are grouped in slices of
 // 32 consecutive rows; a slice stores its rows' edges column-major, entry k
@@ -224,19 +224,21 @@ __device__ __forceinline__ float gain_controller(float g, float r, float dt,
 // launch is never read by it (see the ring note at the top).
 __device__ __forceinline__ float ld_ring(const float *p) { return __ldg(p); }
 
-// Float index of slot `slot` of node `col` in a network's ring: slot pairs
-// (2m, 2m+1) interleaved per node.  A warp's gather of 32 consecutive nodes
-// in one slot still reads whole 32-byte sectors (each holding both slots of
-// four nodes), and the second walk of a pair launch, which reads slot
-// t+1-d where the first read t-d, hits the same word when t-d is even.
-// Measured at N = 10^6, k = 32: 284 us per pair launch against 307 with
-// slot-major rows.  slot * Np + col < 2^32 is checked at creation.
+// Float index of slot `slot` of node `col` in a network's ring: groups of
+// four slots (4m .. 4m+3) of a node side by side (16 bytes).  The second
+// walk of a pair launch reads slot t+1-d where the first read t-d; they
+// share a group unless t-d = 3 mod 4, so three quarters of the second
+// walk's gathers -- the rewired edges' DRAM misses included -- find the word
+// the first walk fetched.  Measured per pair launch at N = 10^6, k = 32:
+// slot-major rows 307 us, pairs of slots 284.7 us, groups of four 277 us,
+// groups of eight 284 us (a warp's gather of 32 consecutive nodes in one
+// slot then spans 32 sectors).  slots * Np < 2^32 is checked at creation.
 __host__ __device__ __forceinline__ unsigned ring_pos(int slot, unsigned col, int Np) {
-  return ((unsigned)(slot >> 1) * (unsigned)Np + col) * 2u + (unsigned)(slot & 1);
+  return ((unsigned)(slot >> 2) * (unsigned)Np + col) * 4u + (unsigned)(slot & 3);
 }
 
-// Slots allocated per node: bsi rounded up to even (whole pairs).
-__host__ __device__ __forceinline__ int ring_slots(int bsi) { return (bsi + 1) & ~1; }
+// Slots allocated per node: bsi rounded up to whole groups of four.
+__host__ __device__ __forceinline__ int ring_slots(int bsi) { return (bsi + 3) & ~3; }
 
 // ---------------------------------------------------------------------------
 // The fused step.
