@@ -720,7 +720,8 @@ def run_reference(args, rank, world, local):
     on the engine's own stream.  ``e2e``: construction from host arrays
     (leviathan_init, :270-389), K steps and ``leviathan_get_theta`` (:440),
     wall clock, with the host<->device bytes declared exactly as for this
-    repository's arm.  The faster of the two reference builds is reported."""
+    repository's arm.  Each metric comes from the faster of the two
+    reference builds at it."""
     if rank != 0:
         return
     import torch
@@ -769,6 +770,7 @@ def run_reference(args, rank, world, local):
         return
     best = max(device, key=device.get)
     v = device[best]
+    best_e2e = min(e2e_s, key=e2e_s.get)  # each metric from the build that is faster at it
     line = {
         "impl": "reference", "metric": "edge-updates/s", "value": v,
         "unit": "edge-updates/s", "n_gpus": 1, "steps": K, "warmup": W,
@@ -779,13 +781,13 @@ def run_reference(args, rank, world, local):
         "timing": "value: CUDA events on the reference engine's stream around K "
                   "leviathan_step calls after construction and W warm-up steps",
         "reference_builds": {"device": device, "e2e_seconds": e2e_s},
-        "reference_build_used": best,
-        "e2e": {"value": E * K / e2e_s[best], "unit": "edge-updates/s",
+        "reference_build_used": best, "reference_build_used_e2e": best_e2e,
+        "e2e": {"value": E * K / e2e_s[best_e2e], "unit": "edge-updates/s",
                 "h2d_bytes_per_step": h2d_bytes(N, E) / K,
                 "d2h_bytes_per_step": d2h_bytes(N, K) / K,
                 "path": "leviathan_init(host arrays) + K x leviathan_step -> r "
                         "+ leviathan_get_theta",
-                "seconds": e2e_s[best], "parts": parts[best]},
+                "seconds": e2e_s[best_e2e], "parts": parts[best_e2e]},
         "gpu_launches": 4 * K,
     }
     print(json.dumps(line), flush=True)
