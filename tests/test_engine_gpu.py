@@ -625,3 +625,26 @@ def test_reference_abi_layer():
     assert lib.leviathan_get_vram_usage(h) > 0
     lib.leviathan_free(h)
     e.close()
+
+
+def test_engine_memory_pool_and_creation_profile():
+    """Engines take their device memory from the library's pool: a freed
+    engine's memory serves the next one; lev_trim_memory returns it to the
+    device, and engines still work afterwards.  The creation profile names
+    every phase with a non-negative time."""
+    from leviathan_v1_b200 import _lib
+
+    lib = _lib.load()
+    net = make_network(20_000, 16, 0.1, 30, seed=31)
+    a = LeviathanEngine(*net.engine_args())
+    prof = a.create_profile()
+    assert len(prof) == 8 and all(v >= 0.0 for v in prof.values())
+    ra = a.step_n(DT, 30)
+    a.close()
+    b = LeviathanEngine(*net.engine_args())  # reuses the pooled memory
+    np.testing.assert_array_equal(b.step_n(DT, 30), ra)
+    b.close()
+    assert lib.lev_trim_memory() == 0
+    c = LeviathanEngine(*net.engine_args())
+    np.testing.assert_array_equal(c.step_n(DT, 30), ra)
+    c.close()
