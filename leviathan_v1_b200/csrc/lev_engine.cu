@@ -1330,14 +1330,6 @@ int create_impl(LevEngine **out, int num_nets, const int32_t *Ns,
       return fail(LEV_ERR_ARG, "network " + std::to_string(n) +
                                    ": row_ptr[0] must be 0");
     }
-    for (int i = 0; i < N; ++i) {
-      if (rp[i + 1] < rp[i]) {
-        delete h;
-        return fail(LEV_ERR_ARG, "network " + std::to_string(n) +
-                                     ": row_ptr is decreasing at row " +
-                                     std::to_string(i));
-      }
-    }
     const long long E = rp[N];
     NetDesc &d = h->h_nets[n];
     std::memset(&d, 0, sizeof(d));
@@ -1370,16 +1362,33 @@ int create_impl(LevEngine **out, int num_nets, const int32_t *Ns,
       return fail(LEV_ERR_ARG, "network " + std::to_string(n) +
                                    ": (max_delay + 2) * N must be below 2^32");
     }
-    // SELL-32 slices: entry k of row i at sl_off[i/32] + 32k + i%32
+    // SELL-32 slices: entry k of row i at sl_off[i/32] + 32k + i%32; the
+    // same pass checks that row_ptr never decreases
     d.slice_base = slices;
-    for (int s0 = 0; s0 < N; s0 += 32) {
-      int len = 0;
-      for (int i = s0; i < std::min(N, s0 + 32); ++i)
-        len = std::max(len, rp[i + 1] - rp[i]);
-      h_sl_off.push_back(sl_total);
-      h_sl_len.push_back(len);
+    const int nsl = (N + 31) / 32;
+    h_sl_off.resize((size_t)(slices + nsl));
+    h_sl_len.resize((size_t)(slices + nsl));
+    int neg = 0;
+    for (int q = 0; q < nsl; ++q) {
+      const int s0 = 32 * q, s1 = std::min(N, s0 + 32);
+      int len = 0, lo = 0;
+      for (int i = s0; i < s1; ++i) {
+        const int deg = rp[i + 1] - rp[i];
+        len = std::max(len, deg);
+        lo = std::min(lo, deg);
+      }
+      neg |= (lo < 0);
+      h_sl_off[(size_t)(slices + q)] = sl_total;
+      h_sl_len[(size_t)(slices + q)] = len;
       sl_total += 32LL * len;
-      ++slices;
+    }
+    slices += nsl;
+    if (neg) {
+      int i = 0;
+      while (rp[i + 1] >= rp[i]) ++i;
+      delete h;
+      return fail(LEV_ERR_ARG, "network " + std::to_string(n) +
+                                   ": row_ptr is decreasing at row " + std::to_string(i));
     }
     h->net_E[n] = E;
     node_off += N;
