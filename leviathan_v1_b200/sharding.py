@@ -69,19 +69,26 @@ def gather_results(local_indices: Sequence[int], local_values: np.ndarray,
 
 def run_sweep(specs, steps: int, dt: float = 0.05, tail: int = 100,
               rank: int = 0, world_size: int = 1, autotune: bool = True,
-              math_mode: str = "reference") -> np.ndarray:
+              math_mode: str = "reference", engine_factory=None) -> np.ndarray:
     """r(K) sweep over ``specs`` (see ``graphs.batch_specs``) sharded over
     ``world_size`` ranks; returns [len(specs), 2] (mean, std of r over the
-    last ``tail`` steps) on every rank."""
-    from .engine import BatchEngine
+    last ``tail`` steps) on every rank.  ``engine_factory(nets, params,
+    math_mode)`` builds a rank's engine (default: a ``BatchEngine``; tests
+    substitute a host stand-in to run the sharding on CPU ranks)."""
     from .graphs import build_batch
+
+    if engine_factory is None:
+        from .engine import BatchEngine
+
+        def engine_factory(nets, params, math_mode):
+            return BatchEngine([n.as_dict() for n in nets], params=params,
+                               math_mode=math_mode)
 
     shards = shard_by_edges([s["E"] for s in specs], world_size)
     mine = shards[rank]
     if mine:
         nets, params = build_batch([specs[i] for i in mine])
-        eng = BatchEngine([n.as_dict() for n in nets], params=params,
-                          math_mode=math_mode)
+        eng = engine_factory(nets, params, math_mode)
         if autotune:
             eng.autotune(dt)
         r = eng.step_n(dt, steps)

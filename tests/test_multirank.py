@@ -87,3 +87,71 @@ def test_gloo_two_ranks_gather_and_reduce():
         for r, s in enumerate(shards):
             assert np.all(out[s, 1] == r)
         assert mx == 11.0 and sm == 3.0
+
+
+class _OracleBatch:
+    """Host stand-in for a rank's BatchEngine: the FP64 oracle per network."""
+
+    def __init__(self, nets, params, math_mode):
+        from oracle64 import OracleEngine
+
+        self.o = [OracleEngine(*n.engine_args(), params=p) for n, p in zip(nets, params)]
+
+    def autotune(self, dt):
+        pass
+
+    def step_n(self, dt, n):
+        return np.stack([o.run(dt, n) for o in self.o], axis=1)  # [steps, nets]
+
+    def close(self):
+        pass
+
+
+SWEEP = dict(num=9, seed=5, n_lo=60, n_hi=300, ks=(4, 6, 8))
+
+
+def _sweep_worker(rank, world, port, q):
+    import torch.distributed as dist
+
+    from leviathan_v1_b200.sharding import run_sweep
+
+    os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port))
+    dist.init_process_group("gloo", rank=rank, world_size=world)
+    try:
+        specs = batch_specs(**SWEEP)
+        out = run_sweep(specs, steps=40, tail=10, rank=rank, world_size=world,
+                        engine_factory=_OracleBatch)
+        q.put((rank, out))
+    finally:
+        dist.destroy_process_group()
+
+
+@pytest.mark.timeout(180)
+def test_gloo_sweep_end_to_end_lands_every_network_in_its_row():
+    """run_sweep sharded over two gloo ranks (a host stand-in engine on each)
+    gives every rank the whole r(K) table, each network's row equal to that
+    network run alone."""
+    from leviathan_v1_b200.graphs import build_batch
+    from leviathan_v1_b200.sharding import run_sweep
+
+    world = 2
+    port = _free_port()
+    ctx = mp.get_context("spawn")
+    q = ctx.Queue()
+    procs = [ctx.Process(target=_sweep_worker, args=(r, world, port, q)) for r in range(world)]
+    for p in procs:
+        p.start()
+    res = dict(q.get(timeout=150) for _ in range(world))
+    for p in procs:
+        p.join(timeout=30)
+        assert p.exitcode == 0
+    specs = batch_specs(**SWEEP)
+    single = run_sweep(specs, steps=40, tail=10, engine_factory=_OracleBatch)
+    nets, params = build_batch(specs)
+    alone = np.stack([summarize_r(_OracleBatch([n], [p], None).step_n(0.05, 40), 10)[0]
+                      for n, p in zip(nets, params)])
+    for r in range(world):
+        np.testing.assert_array_equal(res[r], single)
+    # (mean/std over a [steps, nets] block or one column: summation order only)
+    np.testing.assert_allclose(single, alone, rtol=1e-12, atol=1e-15)
+    assert len(set(map(tuple, shard_by_edges([s["E"] for s in specs], world)))) == world
