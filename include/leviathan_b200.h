@@ -129,10 +129,11 @@ int lev_trim_memory(void);
  * reference counterpart; for tuning construction): ms_out[8] = host-side
  * validation and layout; stream and kernel set-up; the one device
  * allocation; the mapped host buffer of r; small uploads (descriptors, tile
- * lists); the staged pass over the caller's arrays (host threads pack the
- * edges into SELL-32 and copy the node arrays into pinned buffers,
- * validating columns and delays, and issue the DMAs); the ring-fill launch;
- * the wait for every DMA and the fill. */
+ * lists) and the temporary device buffer of the CSR edge arrays; the staged
+ * pass over the caller's arrays (host threads copy them into pinned buffers
+ * and issue the DMAs); the launches of the SELL-32 packing (which validates
+ * columns and delays) and of the ring fill; the wait for every DMA, the
+ * packing and the fill. */
 int lev_create_profile(const LevEngine *h, double *ms_out);
 
 /* Shape queries. */

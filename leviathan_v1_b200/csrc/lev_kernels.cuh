@@ -538,6 +538,65 @@ __global__ void sell_convert_kernel(int mode, const int *__restrict__ row_ptr,
   }
 }
 
+// CSR -> SELL-32 of every network of an engine at creation, one warp per
+// slice: lane l takes row l of the slice and writes its entries k = 0 ..
+// len-1 (len: the slice's longest row) at sl_off[s] + 32k + l, so each k is
+// one contiguous 128-byte store per warp; entries past the row's degree are
+// padding (node 0, delay 0, weight 0: read, never used).  The CSR arrays
+// (concatenated over networks, as the caller passed them) were copied to the
+// device as they are.  Validation as sell_convert_kernel: bit 1 a column
+// outside [0, ncols) (ncols = N, plus the halo columns of a partition for
+// network 0), bit 2 a delay above max_delay, bit 4 a zero delay (not an
+// error: it rules out two steps per launch).
+__global__ void sell_pack_kernel(const NetDesc *__restrict__ nets,
+                                 const int *__restrict__ slice_net, long long slices,
+                                 const long long *__restrict__ sl_off,
+                                 const int *__restrict__ sl_len,
+                                 const int *__restrict__ row_ptr,
+                                 const int *__restrict__ col,
+                                 const uint8_t *__restrict__ delays,
+                                 const float *__restrict__ w, int n_ext,
+                                 uint32_t *__restrict__ sl_cd, float *__restrict__ sl_w,
+                                 unsigned *__restrict__ err) {
+  const int lane = threadIdx.x & 31;
+  const long long warp0 = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const long long nwarps = ((long long)gridDim.x * blockDim.x) >> 5;
+  unsigned bad = 0u;
+  for (long long s = warp0; s < slices; s += nwarps) {  // warp-uniform
+    const int n = slice_net[s];
+    const NetDesc &nd = nets[n];
+    const int N = nd.N;
+    const int row = (int)(s - nd.slice_base) * 32 + lane;
+    const unsigned ncols = (unsigned)(N + (n == 0 ? n_ext : 0));
+    const unsigned md = (unsigned)nd.max_delay;
+    int e0 = 0, deg = 0;
+    if (row < N) {
+      const int *rp = row_ptr + nd.rp_off + row;
+      e0 = rp[0];
+      deg = rp[1] - e0;
+    }
+    const long long eb = nd.edge_off + e0;
+    const long long base = sl_off[s] + lane;
+    const int len = sl_len[s];
+    for (int k = 0; k < len; ++k) {
+      uint32_t word = 0u;
+      float wv = 0.0f;
+      if (k < deg) {
+        const int c = col[eb + k];
+        const unsigned d = delays[eb + k];
+        bad |= (unsigned)((unsigned)c >= ncols) | ((unsigned)(d > md) << 1) |
+               ((unsigned)(d == 0u) << 2);
+        word = ((uint32_t)c << 8) | d;
+        wv = w[eb + k];
+      }
+      sl_cd[base + 32LL * k] = word;
+      sl_w[base + 32LL * k] = wv;
+    }
+  }
+  bad = __reduce_or_sync(0xffffffffu, bad);
+  if (lane == 0 && bad) atomicOr(err, bad);
+}
+
 // r-history row counters := 0 (first node of every captured step block).
 __global__ void reset_rpos_kernel(NetState *st, int num_nets) {
   for (int n = blockIdx.x * blockDim.x + threadIdx.x; n < num_nets;

@@ -312,7 +312,7 @@ class _EngineBase:
         ms = (C.c_double * 8)()
         check(self._lib.lev_create_profile(self.handle, ms))
         keys = ("layout", "stream_and_kernel_setup", "device_allocation", "mapped_host_buffer",
-                "small_uploads", "staged_uploads", "fill_launch", "dma_wait")
+                "small_uploads", "staged_uploads", "pack_and_fill_launch", "dma_wait")
         return {k: float(v) for k, v in zip(keys, ms)}
 
     def set_grid_wait(self, limit_ns: int = 2_000_000_000, extra_arrivals: int = 0) -> None:

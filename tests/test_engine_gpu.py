@@ -595,11 +595,22 @@ def test_invalid_topology_rejected_on_device():
     with pytest.raises(ValueError, match="col_idx"):
         LeviathanEngine(net.N, 10, net.row_ptr, col, net.delays, net.weights,
                         net.theta, net.theta_hat, net.omega)
+    col[17] = -3
+    with pytest.raises(ValueError, match="col_idx"):
+        LeviathanEngine(net.N, 10, net.row_ptr, col, net.delays, net.weights,
+                        net.theta, net.theta_hat, net.omega)
     d = net.delays.copy()
     d[3] = 11
     with pytest.raises(ValueError, match="delay"):
         LeviathanEngine(net.N, 10, net.row_ptr, net.col_idx, d, net.weights,
                         net.theta, net.theta_hat, net.omega)
+    # in a batch, each network's columns are checked against its own N
+    small = make_network(300, 8, 0.1, 10, seed=2)
+    bad = small.as_dict()
+    bad["col_idx"] = bad["col_idx"].copy()
+    bad["col_idx"][-1] = 300  # valid in the first network (N = 500), not here
+    with pytest.raises(ValueError, match="col_idx"):
+        BatchEngine([net.as_dict(), bad])
 
 
 def test_reference_abi_layer():
