@@ -127,13 +127,14 @@ int lev_trim_memory(void);
 
 /* Wall-clock milliseconds of the phases of the engine's creation (no
  * reference counterpart; for tuning construction): ms_out[8] = host-side
- * validation and layout; stream and kernel set-up; the one device
- * allocation; the mapped host buffer of r; small uploads (descriptors, tile
- * lists) and the temporary device buffer of the CSR edge arrays; the staged
- * pass over the caller's arrays (host threads copy them into pinned buffers
- * and issue the DMAs); the launches of the SELL-32 packing (which validates
- * columns and delays) and of the ring fill; the wait for every DMA, the
- * packing and the fill. */
+ * validation and layout, and kernel set-up (both on a helper thread, while
+ * the caller's CSR edge arrays are already being staged to a temporary
+ * device buffer); the stream and the device allocations; the mapped host
+ * buffer of r; small uploads (descriptors, tile lists); the staged pass (the
+ * edge arrays, overlapping the first two phases, then the node arrays: host
+ * threads copy them into pinned buffers and issue the DMAs); the launches
+ * of the SELL-32 packing (which validates columns and delays) and of the
+ * ring fill; the wait for every DMA, the packing and the fill. */
 int lev_create_profile(const LevEngine *h, double *ms_out);
 
 /* Shape queries. */

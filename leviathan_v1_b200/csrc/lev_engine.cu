@@ -1255,184 +1255,55 @@ int create_impl(LevEngine **out, int num_nets, const int32_t *Ns,
   if (math_mode != LEV_MATH_REFERENCE && math_mode != LEV_MATH_ACCURATE)
     return fail(LEV_ERR_ARG, "math_mode must be 0 (reference) or 1");
 
+  // ---- scalar arguments and sizes from the ends of row_ptr, before any
+  // device work: the edge arrays then start moving to the device at once,
+  // while a helper thread lays out the engine (a pass over row_ptr that also
+  // checks it never decreases) and sets up its kernels
+  long long e_total = 0, s_total = 0;
+  {
+    long long ro = 0;
+    for (int n = 0; n < num_nets; ++n) {
+      const int N = Ns[n], md = mds[n];
+      if (N < 1 || N >= (1 << 24))
+        return fail(LEV_ERR_ARG, "network " + std::to_string(n) +
+                                     ": N must be in [1, 2^24), got " + std::to_string(N));
+      if (md < 0 || md > 255)
+        return fail(LEV_ERR_ARG, "network " + std::to_string(n) +
+                                     ": max_delay must be in [0,255] (uint8 delays), got " +
+                                     std::to_string(md));
+      if (rp_cat[ro] != 0)
+        return fail(LEV_ERR_ARG, "network " + std::to_string(n) + ": row_ptr[0] must be 0");
+      const long long E = rp_cat[ro + N];
+      if (E < 0)
+        return fail(LEV_ERR_ARG, "network " + std::to_string(n) + ": row_ptr[N] is negative");
+      LevParams p;
+      if (params) p = params[n]; else lev_default_params(&p);
+      const int prc = check_params(p);
+      if (prc != LEV_OK) return prc;
+      e_total += E;
+      s_total += (N + 31) / 32;
+      ro += N + 1;
+    }
+  }
+  if (e_total > 0 && (!col_cat || !d_cat || !w_cat))
+    return fail(LEV_ERR_ARG, "null edge array argument");
+
   const auto t_start = std::chrono::steady_clock::now();
   double t_mark = 0.0;
   LevEngine *h = new LevEngine();
-  auto mark = [&](int k) {
-    const double t = ms_since(t_start);
-    h->create_ms[k] = t - t_mark;
+  auto lap = [&]() {
+    const double t = ms_since(t_start), d = t - t_mark;
     t_mark = t;
+    return d;
   };
   h->num_nets = num_nets;
   h->math_mode = math_mode;
   h->h_nets.resize(num_nets);
   h->net_E.resize(num_nets);
-
-  // ---- validate shapes and lay out the packed arrays ----------------------
-  long long node_off = 0, edge_off = 0, ring_off = 0, rp_off = 0;
-  long long slices = 0, sl_total = 0;
-  std::vector<long long> h_sl_off;
-  std::vector<int> h_sl_len;
-  int tiles = 0;
-  for (int n = 0; n < num_nets; ++n) {
-    const int N = Ns[n], md = mds[n];
-    if (N < 1 || N >= (1 << 24)) {
-      delete h;
-      return fail(LEV_ERR_ARG, "network " + std::to_string(n) +
-                                   ": N must be in [1, 2^24), got " +
-                                   std::to_string(N));
-    }
-    if (md < 0 || md > 255) {
-      delete h;
-      return fail(LEV_ERR_ARG, "network " + std::to_string(n) +
-                                   ": max_delay must be in [0,255] (uint8 "
-                                   "delays), got " + std::to_string(md));
-    }
-    const int32_t *rp = rp_cat + rp_off;
-    if (rp[0] != 0) {
-      delete h;
-      return fail(LEV_ERR_ARG, "network " + std::to_string(n) +
-                                   ": row_ptr[0] must be 0");
-    }
-    const long long E = rp[N];
-    NetDesc &d = h->h_nets[n];
-    std::memset(&d, 0, sizeof(d));
-    d.node_off = node_off;
-    d.edge_off = edge_off;
-    d.ring_off = ring_off;
-    d.rp_off = rp_off;
-    d.N = N;
-    if ((long long)N + n_ext >= (1LL << 24)) {
-      delete h;
-      return fail(LEV_ERR_ARG, "N plus halo nodes must be below 2^24");
-    }
-    d.Np = (N + n_ext + 31) / 32 * 32;
-    d.bsi = md + 2;
-    d.max_delay = md;
-    d.ntiles = (N + kTile - 1) / kTile;
-    d.part_off = tiles;
-    d.tile_off = tiles;
-    LevParams p;
-    if (params) p = params[n]; else lev_default_params(&p);
-    int rc = check_params(p);
-    if (rc != LEV_OK) {
-      delete h;
-      return rc;
-    }
-    params_to_desc(p, &d);
-    // ring gathers index a network's ring with 32-bit slot * Np + col
-    if ((unsigned long long)ring_slots(d.bsi) * (unsigned long long)d.Np >= (1ull << 32)) {
-      delete h;
-      return fail(LEV_ERR_ARG, "network " + std::to_string(n) +
-                                   ": (max_delay + 2) * N must be below 2^32");
-    }
-    // SELL-32 slices: entry k of row i at sl_off[i/32] + 32k + i%32; the
-    // same pass checks that row_ptr never decreases
-    d.slice_base = slices;
-    const int nsl = (N + 31) / 32;
-    h_sl_off.resize((size_t)(slices + nsl));
-    h_sl_len.resize((size_t)(slices + nsl));
-    int neg = 0;
-    for (int q = 0; q < nsl; ++q) {
-      const int s0 = 32 * q, s1 = std::min(N, s0 + 32);
-      int len = 0, lo = 0;
-      for (int i = s0; i < s1; ++i) {
-        const int deg = rp[i + 1] - rp[i];
-        len = std::max(len, deg);
-        lo = std::min(lo, deg);
-      }
-      neg |= (lo < 0);
-      h_sl_off[(size_t)(slices + q)] = sl_total;
-      h_sl_len[(size_t)(slices + q)] = len;
-      sl_total += 32LL * len;
-    }
-    slices += nsl;
-    if (neg) {
-      int i = 0;
-      while (rp[i + 1] >= rp[i]) ++i;
-      delete h;
-      return fail(LEV_ERR_ARG, "network " + std::to_string(n) +
-                                   ": row_ptr is decreasing at row " + std::to_string(i));
-    }
-    h->net_E[n] = E;
-    node_off += N;
-    edge_off += E;
-    ring_off += (long long)ring_slots(d.bsi) * d.Np;
-    rp_off += N + 1;
-    tiles += d.ntiles;
-  }
-  if (edge_off > 0 && (!col_cat || !d_cat || !w_cat)) {
-    delete h;
-    return fail(LEV_ERR_ARG, "null edge array argument");
-  }
-  h_sl_off.push_back(sl_total);  // end of the last slice (packing jobs)
-  std::vector<int> slice_net((size_t)slices);
-  for (int n = 0; n < num_nets; ++n) {
-    const NetDesc &d = h->h_nets[n];
-    const long long ns = (d.N + 31) / 32;
-    for (long long k = 0; k < ns; ++k) slice_net[(size_t)(d.slice_base + k)] = n;
-  }
-  h->total_nodes = node_off;
-  h->total_edges = edge_off;
-  h->num_slices = slices;
-  h->sl_total = sl_total;
-  h->rp_total = rp_off;
-  h->ring_floats = ring_off;
-  h->total_tiles = tiles;
-
-  // Tile list grouped by degree class (class = mean SELL slice length of the
-  // network); within a class, networks keep their order.
-  std::vector<int> net_class(num_nets);
-  for (int n = 0; n < num_nets; ++n) {
-    const NetDesc &d = h->h_nets[n];
-    const long long s0 = d.slice_base, ns = (d.N + 31) / 32;
-    double sum = 0.0;
-    for (long long s = s0; s < s0 + ns; ++s) sum += h_sl_len[s];
-    const double mean = ns ? sum / ns : 0.0;
-    net_class[n] = degree_class(mean);
-    TileClass &tc = h->classes[net_class[n]];
-    tc.mean_len = (tc.mean_len * tc.ntiles + mean * d.ntiles) /
-                  std::max(1, tc.ntiles + d.ntiles);
-    tc.ntiles += d.ntiles;
-    tc.edges += h->net_E[n];
-  }
-  for (int c = 1; c < kNumClasses; ++c)
-    h->classes[c].tile_off = h->classes[c - 1].tile_off + h->classes[c - 1].ntiles;
-  std::vector<int> h_class_nets;
-  for (int c = 0; c < kNumClasses; ++c) {
-    h->classes[c].net_off = (int)h_class_nets.size();
-    for (int n = 0; n < num_nets; ++n)
-      if (net_class[n] == c) h_class_nets.push_back(n);
-    h->classes[c].nnets = (int)h_class_nets.size() - h->classes[c].net_off;
-  }
-  std::vector<int2> h_tiles(tiles);
-  {
-    int fill[kNumClasses];
-    for (int c = 0; c < kNumClasses; ++c) fill[c] = h->classes[c].tile_off;
-    for (int n = 0; n < num_nets; ++n) {
-      const NetDesc &d = h->h_nets[n];
-      for (int t = 0; t < d.ntiles; ++t)
-        h_tiles[fill[net_class[n]]++] = make_int2(n, t * kTile);
-    }
-  }
-  {
-    // remembered choices of earlier engines with a similar class
-    std::lock_guard<std::mutex> lk(g_tune_mu);
-    for (int c = 0; c < kNumClasses; ++c) {
-      auto it = g_tune_cache.find(tune_key(h->classes[c], c));
-      h->classes[c].variant = (it != g_tune_cache.end()) ? it->second : 0;
-      auto ip = g_pair_cache.find(tune_key(h->classes[c], c));
-      h->classes[c].pair_variant = (ip != g_pair_cache.end()) ? ip->second : 0;
-    }
-  }
-
-  mark(0);
-  // ---- device resources ----------------------------------------------------
   cudaError_t ce = cudaGetDevice(&h->device);
   if (ce != cudaSuccess) {
     delete h;
-    return fail(LEV_ERR_CUDA,
-                std::string("no CUDA device: ") + cudaGetErrorString(ce));
+    return fail(LEV_ERR_CUDA, std::string("no CUDA device: ") + cudaGetErrorString(ce));
   }
   ce = cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking);
   if (ce != cudaSuccess) {
@@ -1440,22 +1311,242 @@ int create_impl(LevEngine **out, int num_nets, const int32_t *Ns,
     return fail(LEV_ERR_CUDA, std::string("cudaStreamCreate failed: ") +
                                   cudaGetErrorString(ce));
   }
-  int rc = prepare_step_kernels();
-  setup_cluster(h, h_sl_off, h_sl_len);
-  if (rc == LEV_OK) rc = setup_grid(h, h_sl_off, h_sl_len);
+  // the temporary device buffer: col [E] | weights [E] | delays [E] |
+  // slice -> network [slices] | error word
+  char *tmp = nullptr;
+  auto cleanup_fail = [&](int code, const std::string &msg) {
+    cudaStreamSynchronize(h->stream);
+    if (tmp) cudaFreeAsync(tmp, h->stream);
+    cudaStreamSynchronize(h->stream);
+    free_engine(h);
+    return fail(code, msg);
+  };
+  const long long E1 = std::max<long long>(e_total, 1);
+  const size_t off_w = (size_t)(4 * E1 + 255) / 256 * 256;
+  const size_t off_dl = off_w + (size_t)(4 * E1 + 255) / 256 * 256;
+  const size_t off_sn = off_dl + (size_t)(E1 + 255) / 256 * 256;
+  const size_t off_err = off_sn + (size_t)(4 * std::max<long long>(s_total, 1) + 255) / 256 * 256;
   {
-    int nbusy = 0;
-    for (int c = 0; c < kNumClasses; ++c) nbusy += h->classes[c].ntiles > 0;
-    if (nbusy > 1) {
-      bool ok = cudaEventCreateWithFlags(&h->ev_fork, cudaEventDisableTiming) == cudaSuccess;
-      for (int c = 0; c < kNumClasses && ok; ++c)
-        ok = cudaStreamCreateWithFlags(&h->class_stream[c], cudaStreamNonBlocking) ==
-                 cudaSuccess &&
-             cudaEventCreateWithFlags(&h->ev_join[c], cudaEventDisableTiming) == cudaSuccess;
-      if (!ok) rc = fail(LEV_ERR_CUDA, "class streams: creation failed");
+    cudaMemPool_t pool = nullptr;
+    cudaError_t e = engine_pool(h->device, &pool);
+    if (e == cudaSuccess)
+      e = cudaMallocFromPoolAsync(reinterpret_cast<void **>(&tmp), off_err + 256, pool,
+                                  h->stream);
+    if (e != cudaSuccess) {
+      cudaGetLastError();
+      tmp = nullptr;
+      return cleanup_fail(LEV_ERR_NOMEM, std::string("device allocation of ") +
+                                             std::to_string(off_err + 256) +
+                                             " bytes failed: " + cudaGetErrorString(e));
     }
   }
-  mark(1);
+  int *t_col = reinterpret_cast<int *>(tmp);
+  float *t_w = reinterpret_cast<float *>(tmp + off_w);
+  uint8_t *t_dl = reinterpret_cast<uint8_t *>(tmp + off_dl);
+  int *t_sn = reinterpret_cast<int *>(tmp + off_sn);
+  unsigned *t_err = reinterpret_cast<unsigned *>(tmp + off_err);
+  double ms_device = lap();
+
+  // ---- validate shapes and lay out the packed arrays (helper thread) -------
+  long long node_off = 0, edge_off = 0, ring_off = 0, rp_off = 0;
+  long long slices = 0, sl_total = 0;
+  std::vector<long long> h_sl_off;
+  std::vector<int> h_sl_len;
+  int tiles = 0;
+  std::vector<int> slice_net;
+  std::vector<int> h_class_nets;
+  std::vector<int2> h_tiles;
+  auto layout = [&]() -> int {
+    for (int n = 0; n < num_nets; ++n) {
+      const int N = Ns[n], md = mds[n];
+      if (N < 1 || N >= (1 << 24)) {
+        return fail(LEV_ERR_ARG, "network " + std::to_string(n) +
+                                     ": N must be in [1, 2^24), got " +
+                                     std::to_string(N));
+      }
+      if (md < 0 || md > 255) {
+        return fail(LEV_ERR_ARG, "network " + std::to_string(n) +
+                                     ": max_delay must be in [0,255] (uint8 "
+                                     "delays), got " + std::to_string(md));
+      }
+      const int32_t *rp = rp_cat + rp_off;
+      if (rp[0] != 0) {
+        return fail(LEV_ERR_ARG, "network " + std::to_string(n) +
+                                     ": row_ptr[0] must be 0");
+      }
+      const long long E = rp[N];
+      NetDesc &d = h->h_nets[n];
+      std::memset(&d, 0, sizeof(d));
+      d.node_off = node_off;
+      d.edge_off = edge_off;
+      d.ring_off = ring_off;
+      d.rp_off = rp_off;
+      d.N = N;
+      if ((long long)N + n_ext >= (1LL << 24)) {
+        return fail(LEV_ERR_ARG, "N plus halo nodes must be below 2^24");
+      }
+      d.Np = (N + n_ext + 31) / 32 * 32;
+      d.bsi = md + 2;
+      d.max_delay = md;
+      d.ntiles = (N + kTile - 1) / kTile;
+      d.part_off = tiles;
+      d.tile_off = tiles;
+      LevParams p;
+      if (params) p = params[n]; else lev_default_params(&p);
+      int rc = check_params(p);
+      if (rc != LEV_OK) {
+        return rc;
+      }
+      params_to_desc(p, &d);
+      // ring gathers index a network's ring with 32-bit slot * Np + col
+      if ((unsigned long long)ring_slots(d.bsi) * (unsigned long long)d.Np >= (1ull << 32)) {
+        return fail(LEV_ERR_ARG, "network " + std::to_string(n) +
+                                     ": (max_delay + 2) * N must be below 2^32");
+      }
+      // SELL-32 slices: entry k of row i at sl_off[i/32] + 32k + i%32; the
+      // same pass checks that row_ptr never decreases
+      d.slice_base = slices;
+      const int nsl = (N + 31) / 32;
+      h_sl_off.resize((size_t)(slices + nsl));
+      h_sl_len.resize((size_t)(slices + nsl));
+      int neg = 0;
+      for (int q = 0; q < nsl; ++q) {
+        const int s0 = 32 * q, s1 = std::min(N, s0 + 32);
+        int len = 0, lo = 0;
+        for (int i = s0; i < s1; ++i) {
+          const int deg = rp[i + 1] - rp[i];
+          len = std::max(len, deg);
+          lo = std::min(lo, deg);
+        }
+        neg |= (lo < 0);
+        h_sl_off[(size_t)(slices + q)] = sl_total;
+        h_sl_len[(size_t)(slices + q)] = len;
+        sl_total += 32LL * len;
+      }
+      slices += nsl;
+      if (neg) {
+        int i = 0;
+        while (rp[i + 1] >= rp[i]) ++i;
+        return fail(LEV_ERR_ARG, "network " + std::to_string(n) +
+                                     ": row_ptr is decreasing at row " + std::to_string(i));
+      }
+      h->net_E[n] = E;
+      node_off += N;
+      edge_off += E;
+      ring_off += (long long)ring_slots(d.bsi) * d.Np;
+      rp_off += N + 1;
+      tiles += d.ntiles;
+    }
+    h_sl_off.push_back(sl_total);  // one more entry: the end of the last slice
+    slice_net.assign((size_t)slices, 0);
+    for (int n = 0; n < num_nets; ++n) {
+      const NetDesc &d = h->h_nets[n];
+      const long long ns = (d.N + 31) / 32;
+      for (long long k = 0; k < ns; ++k) slice_net[(size_t)(d.slice_base + k)] = n;
+    }
+    h->total_nodes = node_off;
+    h->total_edges = edge_off;
+    h->num_slices = slices;
+    h->sl_total = sl_total;
+    h->rp_total = rp_off;
+    h->ring_floats = ring_off;
+    h->total_tiles = tiles;
+
+    // Tile list grouped by degree class (class = mean SELL slice length of the
+    // network); within a class, networks keep their order.
+    std::vector<int> net_class(num_nets);
+    for (int n = 0; n < num_nets; ++n) {
+      const NetDesc &d = h->h_nets[n];
+      const long long s0 = d.slice_base, ns = (d.N + 31) / 32;
+      double sum = 0.0;
+      for (long long s = s0; s < s0 + ns; ++s) sum += h_sl_len[s];
+      const double mean = ns ? sum / ns : 0.0;
+      net_class[n] = degree_class(mean);
+      TileClass &tc = h->classes[net_class[n]];
+      tc.mean_len = (tc.mean_len * tc.ntiles + mean * d.ntiles) /
+                    std::max(1, tc.ntiles + d.ntiles);
+      tc.ntiles += d.ntiles;
+      tc.edges += h->net_E[n];
+    }
+    for (int c = 1; c < kNumClasses; ++c)
+      h->classes[c].tile_off = h->classes[c - 1].tile_off + h->classes[c - 1].ntiles;
+    for (int c = 0; c < kNumClasses; ++c) {
+      h->classes[c].net_off = (int)h_class_nets.size();
+      for (int n = 0; n < num_nets; ++n)
+        if (net_class[n] == c) h_class_nets.push_back(n);
+      h->classes[c].nnets = (int)h_class_nets.size() - h->classes[c].net_off;
+    }
+    h_tiles.assign(tiles, make_int2(0, 0));
+    {
+      int fill[kNumClasses];
+      for (int c = 0; c < kNumClasses; ++c) fill[c] = h->classes[c].tile_off;
+      for (int n = 0; n < num_nets; ++n) {
+        const NetDesc &d = h->h_nets[n];
+        for (int t = 0; t < d.ntiles; ++t)
+          h_tiles[fill[net_class[n]]++] = make_int2(n, t * kTile);
+      }
+    }
+    {
+      // remembered choices of earlier engines with a similar class
+      std::lock_guard<std::mutex> lk(g_tune_mu);
+      for (int c = 0; c < kNumClasses; ++c) {
+        auto it = g_tune_cache.find(tune_key(h->classes[c], c));
+        h->classes[c].variant = (it != g_tune_cache.end()) ? it->second : 0;
+        auto ip = g_pair_cache.find(tune_key(h->classes[c], c));
+        h->classes[c].pair_variant = (ip != g_pair_cache.end()) ? ip->second : 0;
+      }
+    }
+
+    return LEV_OK;
+  };
+  int lrc = LEV_OK;
+  std::string lmsg;
+  std::thread helper([&] {
+    auto t0 = std::chrono::steady_clock::now();
+    cudaError_t e = cudaSetDevice(h->device);
+    lrc = e == cudaSuccess ? layout()
+                           : fail(LEV_ERR_CUDA, std::string("cudaSetDevice failed: ") +
+                                                    cudaGetErrorString(e));
+    h->create_ms[0] = ms_since(t0);
+    t0 = std::chrono::steady_clock::now();
+    if (lrc == LEV_OK) lrc = prepare_step_kernels();
+    if (lrc == LEV_OK) {
+      setup_cluster(h, h_sl_off, h_sl_len);
+      lrc = setup_grid(h, h_sl_off, h_sl_len);
+    }
+    if (lrc == LEV_OK) {
+      int nbusy = 0;
+      for (int c = 0; c < kNumClasses; ++c) nbusy += h->classes[c].ntiles > 0;
+      if (nbusy > 1) {
+        bool ok = cudaEventCreateWithFlags(&h->ev_fork, cudaEventDisableTiming) == cudaSuccess;
+        for (int c = 0; c < kNumClasses && ok; ++c)
+          ok = cudaStreamCreateWithFlags(&h->class_stream[c], cudaStreamNonBlocking) ==
+                   cudaSuccess &&
+               cudaEventCreateWithFlags(&h->ev_join[c], cudaEventDisableTiming) == cudaSuccess;
+        if (!ok) lrc = fail(LEV_ERR_CUDA, "class streams: creation failed");
+      }
+    }
+    h->create_ms[1] = ms_since(t0);
+    if (lrc != LEV_OK) lmsg = g_last_error;
+  });
+  // ---- meanwhile: the edge arrays as they are, through the staging buffers
+  cudaError_t se;
+  {
+    std::vector<StageJob> jobs;
+    add_copy_jobs(jobs, 0, t_col, col_cat, sizeof(int32_t) * e_total);
+    add_copy_jobs(jobs, 0, t_w, w_cat, sizeof(float) * e_total);
+    add_copy_jobs(jobs, 0, t_dl, d_cat, sizeof(uint8_t) * e_total);
+    se = run_stage_jobs(jobs, h->stream);
+  }
+  helper.join();
+  double ms_staged = lap();
+  if (lrc != LEV_OK) return cleanup_fail(lrc, lmsg);
+  if (se != cudaSuccess)
+    return cleanup_fail(LEV_ERR_CUDA, std::string("upload failed: ") + cudaGetErrorString(se));
+  if (edge_off != e_total || slices != s_total)
+    return cleanup_fail(LEV_ERR_ARG, "row_ptr changed during creation");
+
+  int rc = LEV_OK;
   // every array sized here in one device allocation (256-byte aligned
   // parts): one cudaMalloc instead of one per array
   {
@@ -1481,7 +1572,7 @@ int create_impl(LevEngine **out, int num_nets, const int32_t *Ns,
     };
     size_t total = 0;
     for (const Part &q : parts) total += (q.bytes + 255) / 256 * 256;
-    if (rc == LEV_OK) {
+    {
       cudaMemPool_t pool = nullptr;
       cudaError_t e = engine_pool(h->device, &pool);
       if (e == cudaSuccess) e = cudaMallocFromPoolAsync(&h->slab, total, pool, h->stream);
@@ -1502,61 +1593,22 @@ int create_impl(LevEngine **out, int num_nets, const int32_t *Ns,
       }
     }
   }
-  if (rc != LEV_OK) {
-    std::string msg = g_last_error;
-    free_engine(h);
-    return fail(rc, msg);
-  }
-  mark(2);
+  if (rc != LEV_OK) return cleanup_fail(rc, g_last_error);
+  ms_device += lap();
   h->h_rmap = mapped_alloc((size_t)num_nets);
   ce = h->h_rmap ? cudaSuccess : cudaErrorMemoryAllocation;
   if (ce == cudaSuccess)
     ce = cudaHostGetDevicePointer(reinterpret_cast<void **>(&h->d_rmap),
                                   h->h_rmap, 0);
-  if (ce != cudaSuccess) {
-    free_engine(h);
-    return fail(LEV_ERR_CUDA, std::string("mapped host buffer: ") +
-                                  cudaGetErrorString(ce));
-  }
+  if (ce != cudaSuccess)
+    return cleanup_fail(LEV_ERR_CUDA, std::string("mapped host buffer: ") +
+                                          cudaGetErrorString(ce));
 
-  mark(3);
-  // ---- uploads: one staged pass over the caller's arrays -------------------
-  // (the CSR edge arrays go to a temporary device buffer as they are and are
-  // packed into SELL-32 and validated there by sell_pack_kernel; the node
-  // arrays are copied in place; all through the same staging buffers)
-  char *tmp = nullptr;
-  auto cleanup_fail = [&](int code, const std::string &msg) {
-    cudaStreamSynchronize(h->stream);
-    if (tmp) cudaFreeAsync(tmp, h->stream);
-    free_engine(h);
-    return fail(code, msg);
-  };
-  // temporary: col [E] | weights [E] | delays [E] | slice -> network [slices]
-  // | error word
-  const long long E = std::max<long long>(edge_off, 1);
-  const size_t off_w = (size_t)(4 * E + 255) / 256 * 256;
-  const size_t off_dl = off_w + (size_t)(4 * E + 255) / 256 * 256;
-  const size_t off_sn = off_dl + (size_t)(E + 255) / 256 * 256;
-  const size_t off_err = off_sn + (size_t)(4 * std::max<long long>(slices, 1) + 255) / 256 * 256;
-  {
-    cudaMemPool_t pool = nullptr;
-    cudaError_t e = engine_pool(h->device, &pool);
-    if (e == cudaSuccess)
-      e = cudaMallocFromPoolAsync(reinterpret_cast<void **>(&tmp), off_err + 256, pool,
-                                  h->stream);
-    if (e != cudaSuccess) {
-      cudaGetLastError();
-      tmp = nullptr;
-      return cleanup_fail(LEV_ERR_NOMEM, std::string("device allocation of ") +
-                                             std::to_string(off_err + 256) +
-                                             " bytes failed: " + cudaGetErrorString(e));
-    }
-  }
-  int *t_col = reinterpret_cast<int *>(tmp);
-  float *t_w = reinterpret_cast<float *>(tmp + off_w);
-  uint8_t *t_dl = reinterpret_cast<uint8_t *>(tmp + off_dl);
-  int *t_sn = reinterpret_cast<int *>(tmp + off_sn);
-  unsigned *t_err = reinterpret_cast<unsigned *>(tmp + off_err);
+  h->create_ms[2] = ms_device;
+  h->create_ms[3] = lap();
+  // ---- uploads: the node arrays through the staging buffers; the edge
+  // arrays, already on the device, are packed into SELL-32 and validated by
+  // sell_pack_kernel
   std::vector<NetState> st(num_nets);
   for (int n = 0; n < num_nets; ++n) {
     std::memset(&st[n], 0, sizeof(NetState));
@@ -1583,20 +1635,17 @@ int create_impl(LevEngine **out, int num_nets, const int32_t *Ns,
     if (e != cudaSuccess)
       return cleanup_fail(LEV_ERR_CUDA, std::string("upload failed: ") + cudaGetErrorString(e));
   }
-  mark(4);
+  h->create_ms[4] = lap();
   {
     std::vector<StageJob> jobs;
     add_copy_jobs(jobs, 0, h->d_row_ptr, rp_cat, sizeof(int32_t) * rp_off);
     add_copy_jobs(jobs, 0, h->d_theta, th_cat, sizeof(float) * node_off);
     add_copy_jobs(jobs, 0, h->d_theta_hat, thh_cat, sizeof(float) * node_off);
     add_copy_jobs(jobs, 0, h->d_omega, om_cat, sizeof(float) * node_off);
-    add_copy_jobs(jobs, 0, t_col, col_cat, sizeof(int32_t) * edge_off);
-    add_copy_jobs(jobs, 0, t_w, w_cat, sizeof(float) * edge_off);
-    add_copy_jobs(jobs, 0, t_dl, d_cat, sizeof(uint8_t) * edge_off);
     cudaError_t e = run_stage_jobs(jobs, h->stream);
     if (e != cudaSuccess)
       return cleanup_fail(LEV_ERR_CUDA, std::string("upload failed: ") + cudaGetErrorString(e));
-    mark(5);
+    h->create_ms[5] = ms_staged + lap();
     // omega_hat starts as omega (leviathan_kernel.cu:350)
     e = cudaMemcpyAsync(h->d_omega_hat, h->d_omega, sizeof(float) * node_off,
                         cudaMemcpyDeviceToDevice, h->stream);
@@ -1616,7 +1665,7 @@ int create_impl(LevEngine **out, int num_nets, const int32_t *Ns,
     int r2 = launch_fill(h, n);
     if (r2 != LEV_OK) return cleanup_fail(r2, g_last_error);
   }
-  mark(6);
+  h->create_ms[6] = lap();
   {
     // waits for the DMAs and the packing (pageable destination)
     unsigned herr = 0u;
@@ -1632,19 +1681,13 @@ int create_impl(LevEngine **out, int num_nets, const int32_t *Ns,
   }
   if (n_ext > 0) {
     int r2 = fill_ext_columns(h, n_ext, theta_ext);
-    if (r2 != LEV_OK) {
-      std::string msg = g_last_error;
-      free_engine(h);
-      return fail(r2, msg);
-    }
+    if (r2 != LEV_OK) return cleanup_fail(r2, g_last_error);
   }
   ce = cudaStreamSynchronize(h->stream);
-  if (ce != cudaSuccess) {
-    free_engine(h);
-    return fail(LEV_ERR_CUDA,
-                std::string("engine init failed: ") + cudaGetErrorString(ce));
-  }
-  mark(7);
+  if (ce != cudaSuccess)
+    return cleanup_fail(LEV_ERR_CUDA,
+                        std::string("engine init failed: ") + cudaGetErrorString(ce));
+  h->create_ms[7] = lap();
   *out = h;
   return LEV_OK;
 }

@@ -308,10 +308,12 @@ class _EngineBase:
         check(self._lib.lev_set_grid_mode(self.handle, 1 if enabled else 0, int(rows_per_cta)))
 
     def create_profile(self) -> dict:
-        """Milliseconds of the phases of this engine's creation."""
+        """Milliseconds of the phases of this engine's creation (``layout``
+        and ``kernel_setup`` run on a helper thread during
+        ``staged_uploads``)."""
         ms = (C.c_double * 8)()
         check(self._lib.lev_create_profile(self.handle, ms))
-        keys = ("layout", "stream_and_kernel_setup", "device_allocation", "mapped_host_buffer",
+        keys = ("layout", "kernel_setup", "stream_and_device_allocation", "mapped_host_buffer",
                 "small_uploads", "staged_uploads", "pack_and_fill_launch", "dma_wait")
         return {k: float(v) for k, v in zip(keys, ms)}
 

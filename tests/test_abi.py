@@ -75,9 +75,11 @@ def _ptr(a):
     (2, 256, None, "max_delay"),
     (2, -1, None, "max_delay"),
     (2, 5, np.array([1, 1, 2], np.int32), "row_ptr[0]"),
-    (2, 5, np.array([0, 2, 1], np.int32), "decreasing"),
 ])
 def test_create_rejects_bad_arguments_before_any_device_work(N, max_delay, rp_fix, msg):
+    """Scalar arguments and the ends of row_ptr.  A decreasing row_ptr is
+    found by the layout pass, which runs while the edge arrays are uploaded
+    (test_engine_gpu.py::test_invalid_row_ptr_and_sizes_rejected)."""
     lib = _lib.load()
     rp, col, d, w, th, om = _tiny()
     if rp_fix is not None:

@@ -189,7 +189,8 @@ def _ref_engine(net, flavor="sm100a"):
 
 @pytest.mark.parametrize("blocks", [False, True], ids=["step", "step_n"])
 @pytest.mark.parametrize("N,k,md,steps", [(20_000, 16, 30, 60), (100_000, 32, 64, 20),
-                                          (1_000_000, 32, 64, 6)])
+                                          (1_000_000, 32, 64, 6),
+                                          (50_000, 16, 255, 300)])  # largest delay; ring wraps
 def test_engine_matches_live_reference(N, k, md, steps, blocks):
     """Against the reference engine itself on the same GPU; ``step_n``
     takes two steps per launch (pair and finish kernels)."""
@@ -241,6 +242,49 @@ def test_error_against_fp64_oracle(mode, tol):
     assert err <= tol, f"{mode}: wrapped phase error {err}"
     assert np.abs(r_eng - r_o).max() <= 10 * tol
     eng.close()
+
+
+def _degenerate(kind):
+    from leviathan_v1_b200.graphs import Network, init_state
+
+    if kind == "no_edges":          # every row empty
+        N, md, rp, col = 777, 9, np.zeros(778, np.int32), np.zeros(0, np.int32)
+    elif kind == "one_node":        # a single node coupled to itself
+        N, md, rp, col = 1, 3, np.array([0, 1], np.int32), np.zeros(1, np.int32)
+    elif kind == "one_node_no_edge":
+        N, md, rp, col = 1, 0, np.zeros(2, np.int32), np.zeros(0, np.int32)
+    else:                           # 33 rows: one full slice and one row more
+        N, md = 33, 5
+        deg = np.arange(N) % 4
+        rp = np.zeros(N + 1, np.int32)
+        np.cumsum(deg, out=rp[1:])
+        col = (np.repeat(np.arange(N), deg) + np.concatenate(
+            [np.arange(1, d + 1) for d in deg])) % N
+        col = col.astype(np.int32)
+    st = init_state(rp, md, 5, delay_lo=min(1, md))
+    return Network(N, md, rp, col, st["delays"], st["weights"], st["theta"],
+                   st["theta_hat"], st["omega"])
+
+
+@pytest.mark.parametrize("kind", ["no_edges", "one_node", "one_node_no_edge", "ragged_33"])
+def test_degenerate_networks_match_fp64_oracle(kind):
+    """Empty edge lists, a single node, and a row count just past one slice,
+    against the FP64 oracle, by single steps and by step blocks."""
+    net = _degenerate(kind)
+    o = OracleEngine(*net.engine_args())
+    r_o = o.run(DT, 60)
+    for blocks in (False, True):
+        eng = LeviathanEngine(*net.engine_args(), math_mode="accurate")
+        if blocks:
+            r = eng.step_n(DT, 60)
+        else:
+            r = np.array([eng.step(DT) for _ in range(60)], np.float32)
+        assert np.abs(r - r_o).max() <= 1e-4, (kind, blocks)
+        assert circular_distance(eng.get_theta(), o.theta).max() <= 1e-4, (kind, blocks)
+        if net.E:
+            assert np.abs(eng.get_weights() - o.w).max() <= 1e-5, (kind, blocks)
+        assert eng.step_count() == 60
+        eng.close()
 
 
 # ---------------------------------------------------------------------------
@@ -611,6 +655,29 @@ def test_invalid_topology_rejected_on_device():
     bad["col_idx"][-1] = 300  # valid in the first network (N = 500), not here
     with pytest.raises(ValueError, match="col_idx"):
         BatchEngine([net.as_dict(), bad])
+
+
+def test_invalid_row_ptr_and_sizes_rejected():
+    """Shape errors found by the host layout pass, which runs while the edge
+    arrays are already on their way to the device: each creation fails with
+    its message, releases what it took, and the next engine is fine."""
+    net = make_network(2000, 8, 0.1, 10, seed=3)
+    args = list(net.engine_args())
+    rp = net.row_ptr.copy()
+    rp[700] = rp[699] - 1  # decreasing at row 699
+    with pytest.raises(ValueError, match="decreasing at row 699"):
+        LeviathanEngine(*(args[:2] + [rp] + args[3:]))
+    rp = net.row_ptr.copy()
+    rp[0] = 1
+    with pytest.raises(ValueError, match="row_ptr\\[0\\]"):
+        LeviathanEngine(*(args[:2] + [rp] + args[3:]))
+    with pytest.raises(ValueError, match="max_delay"):
+        LeviathanEngine(*([net.N, 256] + args[2:]))
+    e = LeviathanEngine(*args)
+    ref = LeviathanEngine(*args)
+    np.testing.assert_array_equal(e.step_n(DT, 20), ref.step_n(DT, 20))
+    e.close()
+    ref.close()
 
 
 def test_reference_abi_layer():
