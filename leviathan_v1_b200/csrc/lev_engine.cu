@@ -192,6 +192,8 @@ struct LevEngine {
   bool spec = false;
   uint32_t spec_dt = 0;  // bits of the dt of the pending step
   float *d_w_spec = nullptr, *d_thh_spec = nullptr, *d_omh_spec = nullptr;
+  void *spec_block = nullptr;  // the three spec buffers: one allocation from the pool
+  size_t spec_bytes = 0;
   int w_flip = 0;
   int *d_class_nets = nullptr;  // networks of each class, class by class
   LevHubs *hubs = nullptr;      // attached hub monitor (lev_attach_hubs)
@@ -375,7 +377,10 @@ void free_engine(LevEngine *h) {
   auto dfree = [h](void *p) {
     const char *c = static_cast<const char *>(p);
     const char *b = static_cast<const char *>(h->slab);
-    if (p && !(b && c >= b && c < b + h->slab_bytes)) cudaFree(p);
+    const char *q = static_cast<const char *>(h->spec_block);
+    if (p && !(b && c >= b && c < b + h->slab_bytes) &&
+        !(q && c >= q && c < q + h->spec_bytes))
+      cudaFree(p);
   };
   dfree(h->d_nets);
   dfree(h->d_st);
@@ -399,6 +404,7 @@ void free_engine(LevEngine *h) {
   dfree(h->d_rhist);
   dfree(h->d_gwsum);
   dfree(h->d_gbar);
+  if (h->spec_block) cudaFreeAsync(h->spec_block, h->stream);
   if (h->slab) cudaFreeAsync(h->slab, h->stream);  // back to the engine pool
   if (h->h_gerr) cudaFreeHost(h->h_gerr);
   mapped_free(h->h_rmap);
@@ -1822,10 +1828,27 @@ int lev_step(LevEngine *h, float dt, float *r_out) {
     } else {
       h->spec = false;
       if (!h->d_w_spec) {
-        rc = dev_alloc(h, &h->d_w_spec, (size_t)std::max<long long>(h->sl_total, 1));
-        if (rc == LEV_OK) rc = dev_alloc(h, &h->d_thh_spec, (size_t)h->total_nodes);
-        if (rc == LEV_OK) rc = dev_alloc(h, &h->d_omh_spec, (size_t)h->total_nodes);
-        if (rc != LEV_OK) return rc;
+        // one block from the engine pool (a driver allocation of this size
+        // costs milliseconds; the pool usually has it from earlier engines)
+        const size_t nw = ((size_t)std::max<long long>(h->sl_total, 1) + 63) / 64 * 64;
+        const size_t nn = ((size_t)std::max<long long>(h->total_nodes, 1) + 63) / 64 * 64;
+        const size_t bytes = sizeof(float) * (nw + 2 * nn);
+        cudaMemPool_t pool = nullptr;
+        cudaError_t e = engine_pool(h->device, &pool);
+        if (e == cudaSuccess) e = cudaMallocFromPoolAsync(&h->spec_block, bytes, pool, h->stream);
+        if (e != cudaSuccess) {
+          cudaGetLastError();
+          h->spec_block = nullptr;
+          return fail(LEV_ERR_NOMEM, std::string("device allocation of ") +
+                                         std::to_string(bytes) + " bytes failed: " +
+                                         cudaGetErrorString(e));
+        }
+        h->spec_bytes = bytes;
+        h->vram += bytes;
+        float *f = static_cast<float *>(h->spec_block);
+        h->d_w_spec = f;
+        h->d_thh_spec = f + nw;
+        h->d_omh_spec = f + nw + nn;
         // padding entries (never written by a walk) as in the live buffer
         LEV_TRY_CUDA(cudaMemcpyAsync(h->d_w_spec, h->d_sl_w,
                                      sizeof(float) * std::max<long long>(h->sl_total, 1),
