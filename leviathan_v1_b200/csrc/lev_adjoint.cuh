@@ -55,6 +55,8 @@ struct AdjFwdArgs {
   float2 *partials;
   const float *drive;  // [total nodes] for this step, or null
   float *thh_rec;      // theta_hat before the step [total nodes], or null
+  float *dj_rec;       // the delayed source phase of every edge this step
+                       // (SELL order, entries below the row's degree), or null
   float4 *trace;       // per network (g used, r, sum cos, sum sin), or null
   float *r_out;        // per network r after the step, or null
   float *theta_out;    // theta after the step [total nodes], or null
@@ -155,6 +157,7 @@ __global__ void __launch_bounds__(kTile, 3) adj_fwd_kernel(const AdjFwdArgs a) {
           if (!isfinite(w)) w = w_min;
           w = fmaxf(w_min, fminf(w_max, w));
           a.w_out[base + 32 * (k0 + u)] = w;
+          if (a.dj_rec) a.dj_rec[base + 32 * (k0 + u)] = delayed_j;
         }
       }
 #pragma unroll
@@ -469,6 +472,7 @@ struct AdjBwdArgs {
   const int *sl_len;
   const uint32_t *sl_cd;
   const float *w_s;    // SELL weights before step s
+  const float *dj_s;   // delayed source phases of step s (SELL), or null: from H
   const float *H;      // history ring: theta(tau) at slot tau - seg_start + max_delay
   const float *thh_s;  // theta_hat before step s [total nodes]
   const float4 *trace; // per network (g_s, r_{s+1}, sum cos, sum sin)
@@ -581,7 +585,9 @@ __global__ void __launch_bounds__(kTile, MINB) adj_bwd_kernel(const AdjBwdArgs a
     const int len = a.sl_len[s];
     const long long base = a.sl_off[s] + lane;
     // all U entries' stream loads, then all gathers, before the dependent
-    // math (measured faster here than a software pipeline of the groups)
+    // math (measured faster here than a software pipeline of the groups).
+    // With dj_s the delayed phases the recompute recorded are one more
+    // stream, so a group waits on memory once instead of twice.
     for (int k0 = 0; k0 < len; k0 += U) {
       uint32_t p[U];
       float wv[U], lw[U], dj[U];
@@ -591,11 +597,14 @@ __global__ void __launch_bounds__(kTile, MINB) adj_bwd_kernel(const AdjBwdArgs a
         p[u] = in ? __ldg(a.sl_cd + base + 32 * (k0 + u)) : 0u;
         wv[u] = in ? a.w_s[base + 32 * (k0 + u)] : 0.0f;
         lw[u] = in ? a.lam_w[base + 32 * (k0 + u)] : 0.0f;
+        if (a.dj_s) dj[u] = in ? __ldcs(a.dj_s + base + 32 * (k0 + u)) : 0.0f;
       }
+      if (!a.dj_s) {
 #pragma unroll
-      for (int u = 0; u < U; ++u) {
-        const int d = (int)(p[u] & 255u);
-        dj[u] = H[(long long)(hs - d) * Np + (p[u] >> 8)];
+        for (int u = 0; u < U; ++u) {
+          const int d = (int)(p[u] & 255u);
+          dj[u] = H[(long long)(hs - d) * Np + (p[u] >> 8)];
+        }
       }
 #pragma unroll
       for (int u = 0; u < U; ++u) {

@@ -3079,6 +3079,10 @@ struct LevAdjoint {
   float *ck_theta = nullptr, *ck_thh = nullptr, *ck_omh = nullptr,
         *ck_w = nullptr, *ck_ring = nullptr, *ck_g = nullptr;
   float *w_hist = nullptr, *thh_hist = nullptr;
+  // delayed source phase of every edge in each step of a segment (SELL),
+  // recorded by the recompute for the reverse steps of the per-step kernels
+  // (grids of more than one wave); null otherwise
+  float *dj_hist = nullptr, *dj_hist2 = nullptr;
   float4 *trace = nullptr;
   // second set of segment records (extended ring, weights, theta_hat, trace)
   // so the backward pass recomputes segment k-1 on `rstream` while segment k
@@ -3544,6 +3548,8 @@ int lev_adj_create(LevAdjoint **out, LevEngine *e, int32_t segment,
   A(a->w_hist, (C + 1) * SL);
   A(a->thh_hist, C * TN);
   A(a->trace, C * NN);
+  const bool dj_rec = e->total_tiles > 148;  // adj_fwd_kernel / adj_bwd_kernel
+  if (dj_rec) A(a->dj_hist, C * SL);
   A(a->lam_th, TN); A(a->lam_thh, TN); A(a->lam_omh, TN);
   A(a->lam_w, SL);
   A(a->adj_ring, a->aux_floats);
@@ -3555,10 +3561,12 @@ int lev_adj_create(LevAdjoint **out, LevEngine *e, int32_t segment,
     // recompute and the reverse steps of each segment one after the other
     size_t fr = 0, tot = 0;
     const size_t need = sizeof(float) * ((size_t)a->ring_floats + (size_t)(C + 1) * SL +
-                                         (size_t)C * TN) + sizeof(float4) * (size_t)C * NN;
+                                         (size_t)C * TN + (dj_rec ? (size_t)C * SL : 0)) +
+                        sizeof(float4) * (size_t)C * NN;
     if (cudaMemGetInfo(&fr, &tot) == cudaSuccess && need + (256ull << 20) < fr) {
       A(a->ring2, a->ring_floats);
       A(a->w_hist2, (C + 1) * SL);
+      if (dj_rec) A(a->dj_hist2, C * SL);
       A(a->thh_hist2, C * TN);
       A(a->trace2, C * NN);
       if (rc == LEV_OK &&
@@ -3827,6 +3835,7 @@ int lev_adj_backward(LevAdjoint *a, const float *dLdr, const float *dLdtheta,
   float *whs[2] = {a->w_hist, overlap ? a->w_hist2 : a->w_hist};
   float *ths[2] = {a->thh_hist, overlap ? a->thh_hist2 : a->thh_hist};
   float4 *trs[2] = {a->trace, overlap ? a->trace2 : a->trace};
+  float *djs[2] = {a->dj_hist, overlap ? a->dj_hist2 : a->dj_hist};
   cudaStream_t rs = overlap ? a->rstream : s;
   if (overlap) {
     LEV_TRY_CUDA(cudaEventRecord(a->ev_start, s));
@@ -3846,6 +3855,7 @@ int lev_adj_backward(LevAdjoint *a, const float *dLdr, const float *dLdtheta,
       f.w_in = whs[buf] + (size_t)k * a->SL;
       f.w_out = whs[buf] + (size_t)(k + 1) * a->SL;
       f.thh_rec = ths[buf] + (size_t)k * a->TN;
+      f.dj_rec = djs[buf] ? djs[buf] + (size_t)k * a->SL : nullptr;
       f.trace = trs[buf] + (size_t)k * a->NN;
       f.drive = a->drive ? a->drive + (size_t)t * a->TN : nullptr;
       f.r_out = nullptr;
@@ -3892,6 +3902,7 @@ int lev_adj_backward(LevAdjoint *a, const float *dLdr, const float *dLdtheta,
       const int k = t - s0;
       b.s = t;
       b.w_s = whs[buf] + (size_t)k * a->SL;
+      b.dj_s = djs[buf] ? djs[buf] + (size_t)k * a->SL : nullptr;
       b.thh_s = ths[buf] + (size_t)k * a->TN;
       b.trace = trs[buf] + (size_t)k * a->NN;
       b.dLdr = dLdr ? dLdr + (size_t)t * a->NN : nullptr;
