@@ -3921,15 +3921,16 @@ int lev_adj_backward(LevAdjoint *a, const float *dLdr, const float *dLdtheta,
         b.grad_rb = a->res_grb;
       }
       // measured on B200: grids of many waves (batch-64 reservoir) run best
-      // at 4 CTAs/SM with 4 edges in flight per lane; a grid of one partial
-      // wave (N = 10^4) with four lanes per row
+      // at 5 CTAs/SM with 6 edges in flight per lane (fwd+bwd 1.75-1.77 s;
+      // 4 CTAs/SM with 4 edges 2.00 s, 6 with 4 1.77 s, 7 or 8 spill: 2.00 s);
+      // a grid of one partial wave (N = 10^4) with four lanes per row
       if (e->total_tiles <= 148) {
         const int g4 = e->total_tiles * 4;
         if (mode) adj_bwd_split_kernel<1, 4, 2><<<g4, kTile, 0, s>>>(b);
         else adj_bwd_split_kernel<0, 4, 2><<<g4, kTile, 0, s>>>(b);
       } else if (e->total_tiles > 3 * 148 * 2) {
-        if (mode) adj_bwd_kernel<1, 4, 4><<<e->total_tiles, kTile, 0, s>>>(b);
-        else adj_bwd_kernel<0, 4, 4><<<e->total_tiles, kTile, 0, s>>>(b);
+        if (mode) adj_bwd_kernel<1, 6, 5><<<e->total_tiles, kTile, 0, s>>>(b);
+        else adj_bwd_kernel<0, 6, 5><<<e->total_tiles, kTile, 0, s>>>(b);
       } else {
         if (mode) adj_bwd_kernel<1, 8, 3><<<e->total_tiles, kTile, 0, s>>>(b);
         else adj_bwd_kernel<0, 8, 3><<<e->total_tiles, kTile, 0, s>>>(b);
