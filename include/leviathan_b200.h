@@ -95,7 +95,10 @@ void lev_default_params(LevParams *p);
  * (init_buffer_kernel, leviathan_kernel.cu:79-90).  max_delay in [0,255]
  * (delays are uint8), N in [1, 2^24).  params may be NULL (defaults).
  * math_mode is LEV_MATH_REFERENCE or LEV_MATH_ACCURATE.  The engine runs on
- * the CUDA device that is current at the call. */
+ * the CUDA device that is current at the call.  The edge arrays are read for
+ * row_ptr[N] entries while the rest of row_ptr is still being checked (as
+ * the reference, which takes E from row_ptr[N], leviathan_kernel.cu:278):
+ * they must hold that many. */
 int lev_create(LevEngine **out, int32_t N, int32_t max_delay,
                const int32_t *row_ptr, const int32_t *col_idx,
                const uint8_t *delays, const float *weights,
