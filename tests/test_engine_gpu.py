@@ -302,6 +302,24 @@ def test_step_n_equals_repeated_step():
     assert a.step_count() == b.step_count() == 300
 
 
+def test_block_issued_directly_then_recorded_then_replayed():
+    """The first block of a length is issued directly, the second records a
+    CUDA graph, the third replays it: all three equal single steps."""
+    net = make_network(30_000, 16, 0.1, 20, seed=12)
+    a = LeviathanEngine(*net.engine_args())
+    b = LeviathanEngine(*net.engine_args())
+    for eng in (a, b):
+        eng.set_cluster_mode(False)
+        eng.set_grid_mode(False)
+    ra = np.array([a.step(DT) for _ in range(3 * 24)], np.float32)
+    rb = np.concatenate([b.step_n(DT, 24) for _ in range(3)])
+    np.testing.assert_array_equal(ra, rb)
+    np.testing.assert_array_equal(a.get_theta(), b.get_theta())
+    np.testing.assert_array_equal(a.get_weights(), b.get_weights())
+    a.close()
+    b.close()
+
+
 @pytest.mark.parametrize("batch", [False, True])
 def test_speculative_single_steps_bit_identical(batch):
     """Single steps run as speculative pairs (the pair kernel's second walk
