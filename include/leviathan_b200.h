@@ -481,6 +481,22 @@ int lev_part_unpack(LevEngine *h, const int32_t *idx_dev, int32_t n,
                     const float *in_dev);
 int lev_part_fill_halo(LevEngine *h, const float *theta_halo);
 
+/* Two steps per pair of launches for a partition (no zero delay, a one-lane
+ * pair variant: lev_part_pairs tells), bitwise the one-step sequence:
+ *   lev_part_pair_begin(partials)  step t in full and step t+1 up to its
+ *                                  integrate; partials of r(t+1)
+ *   all-gather, lev_part_step_end  r(t+1), g(t+1) on every rank
+ *   lev_part_pack, send/recv, lev_part_unpack   theta(t+1) into the halo
+ *                                  (before the finish overwrites theta)
+ *   lev_part_pair_finish(partials) the integrate of step t+1; partials of
+ *                                  r(t+2)
+ *   all-gather, lev_part_step_end  r(t+2), g(t+2)
+ *   lev_part_pack, send/recv, lev_part_unpack   theta(t+2) into the halo.
+ * The next pair reads halo slots t+1 and t+2 only (no delay is 0). */
+int lev_part_pairs(const LevEngine *h, int32_t *eligible);
+int lev_part_pair_begin(LevEngine *h, float dt, void *partials_dev);
+int lev_part_pair_finish(LevEngine *h, float dt, void *partials_dev);
+
 /* ------------------------------------------------------------------------ */
 /* Allocation-free step                                                      */
 /* ------------------------------------------------------------------------ */

@@ -149,6 +149,9 @@ PROTOTYPES = {
     "lev_part_step_begin": (C.c_int, [_P, _f32, _P]),
     "lev_part_step_end": (C.c_int, [_P, _f32, _P, _P]),
     "lev_part_pack": (C.c_int, [_P, _P, _i32, _P]),
+    "lev_part_pairs": (C.c_int, [_P, C.POINTER(_i32)]),
+    "lev_part_pair_begin": (C.c_int, [_P, _f32, _P]),
+    "lev_part_pair_finish": (C.c_int, [_P, _f32, _P]),
     "lev_part_unpack": (C.c_int, [_P, _P, _i32, _P]),
     "lev_part_fill_halo": (C.c_int, [_P, _P]),
     "lev_gen_ws": (C.c_int, [_i32, _i32, C.c_double, C.c_uint64, _i32, _i32, _f32,

@@ -4103,9 +4103,9 @@ int lev_part_create(LevEngine **out, int32_t N, int32_t n_halo, int32_t max_dela
   h->part_N_global = N_global;
   h->part_tile_off = tile_off_global;
   h->part_ntiles_global = ntiles_global;
-  // one step per launch with a host-driven reduction: none of the block paths
-  h->pair_ok = false;
-  h->use_pairs = false;
+  // steps driven by the host (lev_part_step_*, lev_part_pair_*) with the
+  // whole-network reduction on gathered partials: none of the block paths;
+  // pair_ok (no zero delay) stays as creation found it
   h->cluster_ok = false;
   h->use_cluster = false;
   h->grid_ok = false;
@@ -4123,7 +4123,7 @@ int lev_part_create(LevEngine **out, int32_t N, int32_t n_halo, int32_t max_dela
   return LEV_OK;
 }
 
-static int part_check(LevEngine *h) {
+static int part_check(const LevEngine *h) {
   if (!h) return fail(LEV_ERR_ARG, "null handle");
   if (!h->part) return fail(LEV_ERR_STATE, "not a partition engine (lev_part_create)");
   return LEV_OK;
@@ -4158,9 +4158,77 @@ int lev_part_step_end(LevEngine *h, float dt, const void *partials_all_dev,
   if (!std::isfinite(dt)) return fail(LEV_ERR_ARG, "dt is not finite");
   if (!partials_all_dev) return fail(LEV_ERR_ARG, "partials buffer is null");
   DeviceScope ds(h->device);
-  part_finish_kernel<<<1, 32, 0, h->stream>>>(
+  part_finish_kernel<<<1, kReduceThreads, 0, h->stream>>>(
       h->d_nets, h->d_st, static_cast<const float2 *>(partials_all_dev),
       h->part_ntiles_global, h->part_N_global, dt, r_dev, h->d_rmap);
+  LEV_TRY_CUDA(cudaGetLastError());
+  return LEV_OK;
+}
+
+// The single degree class of a partition engine that takes two steps per
+// launch with a one-lane pair variant, or -1.
+static int part_pair_class(const LevEngine *h) {
+  if (!pairs_all(h)) return -1;
+  for (int c = 0; c < kNumClasses; ++c) {
+    const TileClass &tc = h->classes[c];
+    if (tc.ntiles > 0) return kPairVariants[tc.pair_variant].LANES == 1 ? c : -1;
+  }
+  return -1;
+}
+
+int lev_part_pairs(const LevEngine *h, int32_t *eligible) {
+  int rc = part_check(h);
+  if (rc != LEV_OK) return rc;
+  if (!eligible) return fail(LEV_ERR_ARG, "null argument");
+  *eligible = part_pair_class(h) >= 0 ? 1 : 0;
+  return LEV_OK;
+}
+
+// Two steps of a partition per pair of launches, as the single engine takes
+// them (lev_pair.cuh), with the whole-network reduction of each step done by
+// lev_part_step_end on the all-gathered partials instead of reduce_kernel.
+int lev_part_pair_begin(LevEngine *h, float dt, void *partials_dev) {
+  int rc = part_check(h);
+  if (rc != LEV_OK) return rc;
+  if (!std::isfinite(dt)) return fail(LEV_ERR_ARG, "dt is not finite");
+  if (!partials_dev) return fail(LEV_ERR_ARG, "partials buffer is null");
+  const int c = part_pair_class(h);
+  if (c < 0) return fail(LEV_ERR_STATE, "partition engine: two steps per launch not eligible");
+  DeviceScope ds(h->device);
+  StepArgs a = make_args(h, dt, nullptr, 0, nullptr);
+  a.partials = static_cast<float2 *>(partials_dev);
+  a.hubs = nullptr;
+  a.reverse = h->sweep;
+  h->sweep ^= 1;
+  const TileClass &tc = h->classes[c];
+  a.tiles = h->d_tiles + tc.tile_off;
+  const int mode = (h->math_mode == LEV_MATH_ACCURATE) ? 1 : 0;
+  void *args[] = {&a};
+  LEV_TRY_CUDA(cudaLaunchKernel(reinterpret_cast<const void *>(kPairVariants[tc.pair_variant].fn[mode]),
+                                dim3(tc.ntiles), dim3(kTile), args, 0, h->stream));
+  return LEV_OK;
+}
+
+int lev_part_pair_finish(LevEngine *h, float dt, void *partials_dev) {
+  int rc = part_check(h);
+  if (rc != LEV_OK) return rc;
+  if (!std::isfinite(dt)) return fail(LEV_ERR_ARG, "dt is not finite");
+  if (!partials_dev) return fail(LEV_ERR_ARG, "partials buffer is null");
+  const int c = part_pair_class(h);
+  if (c < 0) return fail(LEV_ERR_STATE, "partition engine: two steps per launch not eligible");
+  DeviceScope ds(h->device);
+  StepArgs a = make_args(h, dt, nullptr, 0, nullptr);
+  a.partials = static_cast<float2 *>(partials_dev);
+  a.hubs = nullptr;
+  a.reverse = h->sweep;
+  h->sweep ^= 1;
+  const TileClass &tc = h->classes[c];
+  a.tiles = h->d_tiles + tc.tile_off;
+  const int blocks = (tc.ntiles + kFinishTiles - 1) / kFinishTiles;
+  if (h->math_mode == LEV_MATH_ACCURATE)
+    finish_kernel<1><<<blocks, kTile, 0, h->stream>>>(a, tc.ntiles);
+  else
+    finish_kernel<0><<<blocks, kTile, 0, h->stream>>>(a, tc.ntiles);
   LEV_TRY_CUDA(cudaGetLastError());
   return LEV_OK;
 }

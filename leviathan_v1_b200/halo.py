@@ -151,6 +151,7 @@ class DistExchange:
         self.group = group
         self.rank = dist.get_rank(group)
         self.world = dist.get_world_size(group)
+        self.nccl = dist.get_backend(group) == "nccl"
 
     def _on(self, stream):
         if stream is None:
@@ -162,9 +163,22 @@ class DistExchange:
     def allgather(self, out, chunk, stream=None):
         """``out`` [world * C, ...] := every rank's ``chunk`` [C, ...] in rank
         order (this rank's own chunk may be a view of ``out``)."""
+        n = chunk.numel()
+        own = out.view(-1)[self.rank * n:(self.rank + 1) * n]
+        in_place = own.data_ptr() == chunk.data_ptr()
+        if self.world == 1:
+            if not in_place:
+                own.copy_(chunk.view(-1))
+            return
         with self._on(stream):
-            parts = list(out.view(self.world, *chunk.shape).unbind(0))
-            self.dist.all_gather(parts, chunk.clone(), group=self.group)
+            if self.nccl:
+                # one collective into `out`; NCCL takes the rank's own slot of
+                # the output as the input (its in-place all-gather)
+                self.dist.all_gather_into_tensor(out.view(-1), own if in_place else
+                                                 chunk.reshape(-1), group=self.group)
+            else:
+                parts = list(out.view(self.world, *chunk.shape).unbind(0))
+                self.dist.all_gather(parts, chunk.clone(), group=self.group)
 
     def exchange(self, sends: dict, recvs: dict, stream=None):
         """Point-to-point: ``sends[peer]`` goes to peer, ``recvs[peer]`` is
@@ -291,6 +305,18 @@ class CudaPartition:
         self._check(self._lib.lev_part_step_end(self.h, float(dt), self._p(partials_all),
                                                 self._p(r_slot)))
 
+    # two steps per pair of launches (see lev_part_pair_begin)
+    def pairs_eligible(self) -> bool:
+        el = C.c_int32()
+        self._check(self._lib.lev_part_pairs(self.h, C.byref(el)))
+        return bool(el.value)
+
+    def pair_begin(self, dt, partials):
+        self._check(self._lib.lev_part_pair_begin(self.h, float(dt), self._p(partials)))
+
+    def pair_finish(self, dt, partials):
+        self._check(self._lib.lev_part_pair_finish(self.h, float(dt), self._p(partials)))
+
     def pack(self, idx, out):
         self._check(self._lib.lev_part_pack(self.h, self._p(idx), int(idx.numel()),
                                             self._p(out)))
@@ -374,10 +400,29 @@ class PartitionedEngine:
         self._recv_buf = {p: self.core.tensor(v.size) for p, v in pr.recv.items()}
         self._r_hist = self.core.tensor(256)
         self.steps = 0
+        # two steps per pair of launches when every rank's core can take
+        # them (no zero delay anywhere: each rank checks its own edges); the
+        # ranks agree through one all-gather, so they issue the same
+        # collectives in the same order
+        ok = hasattr(self.core, "pair_begin") and self.core.pairs_eligible()
+        flags = self.core.tensor(world)
+        flags[rank:rank + 1].fill_(1.0 if ok else 0.0)
+        self.exchange.allgather(flags, flags[rank:rank + 1].clone(), stream=None)
+        self._pairs_ok = bool(flags.min().item() > 0.0)
+        self._pairs = self._pairs_ok
 
     @property
     def stream(self):
         return getattr(self.core, "stream", None)
+
+    def _halo(self):
+        """theta after the last step -> the peers' halo columns of its slot."""
+        core, ex, st = self.core, self.exchange, self.stream
+        for p, idx in self._send_idx.items():
+            core.pack(idx, self._send_buf[p])
+        ex.exchange(self._send_buf, self._recv_buf, stream=st)
+        for p, idx in self._recv_idx.items():
+            core.unpack(idx, self._recv_buf[p])
 
     def _one_step(self, dt, r_slot):
         core, ex, st = self.core, self.exchange, self.stream
@@ -385,20 +430,41 @@ class PartitionedEngine:
         core.step_begin(dt, self._part_all)
         ex.allgather(self._part_all, self._chunk, stream=st)
         core.step_end(dt, self._part_all, r_slot)
-        for p, idx in self._send_idx.items():
-            core.pack(idx, self._send_buf[p])
-        ex.exchange(self._send_buf, self._recv_buf, stream=st)
-        for p, idx in self._recv_idx.items():
-            core.unpack(idx, self._recv_buf[p])
+        self._halo()
         self.steps += 1
+
+    def _one_pair(self, dt, r_slots):
+        """Steps t, t+1 (lev_part_pair_begin): the halo gets theta(t+1)
+        before the finish overwrites it, then theta(t+2)."""
+        core, ex, st = self.core, self.exchange, self.stream
+        core.pair_begin(dt, self._part_all)
+        ex.allgather(self._part_all, self._chunk, stream=st)
+        core.step_end(dt, self._part_all, r_slots[0:1])
+        self._halo()
+        core.pair_finish(dt, self._part_all)
+        ex.allgather(self._part_all, self._chunk, stream=st)
+        core.step_end(dt, self._part_all, r_slots[1:2])
+        self._halo()
+        self.steps += 2
+
+    def set_pair_mode(self, enabled: bool) -> None:
+        """Two steps per pair of launches (when every rank can), or one step
+        per launch.  Every rank must make the same call."""
+        self._pairs = bool(enabled) and self._pairs_ok
 
     def step_n(self, dt, n) -> np.ndarray:
         """``n`` steps; returns r of every step (the same on every rank)."""
         n = int(n)
         if self._r_hist.numel() < n:
             self._r_hist = self.core.tensor(n)
-        for k in range(n):
-            self._one_step(dt, self._r_hist[k:k + 1])
+        k = 0
+        while k < n:
+            if self._pairs and k + 1 < n:
+                self._one_pair(dt, self._r_hist[k:k + 2])
+                k += 2
+            else:
+                self._one_step(dt, self._r_hist[k:k + 1])
+                k += 1
         self.core.synchronize()
         return self._r_hist[:n].cpu().numpy().copy()
 

@@ -203,8 +203,9 @@ def test_gloo_partitioned_equals_unpartitioned(world):
 # GPU: CUDA partition engines on one device
 # ---------------------------------------------------------------------------
 @pytest.mark.gpu
+@pytest.mark.parametrize("pairs", [True, False], ids=["pairs", "single"])
 @pytest.mark.parametrize("world,math_mode", [(2, "reference"), (3, "accurate")])
-def test_cuda_partitions_equal_single_engine(world, math_mode):
+def test_cuda_partitions_equal_single_engine(world, math_mode, pairs):
     if not has_gpu():
         pytest.fail("needs a CUDA device")
     from leviathan_v1_b200 import LeviathanEngine
@@ -233,6 +234,8 @@ def test_cuda_partitions_equal_single_engine(world, math_mode):
             torch.cuda.set_device(0)
             e = PartitionedEngine(r, world, *net.engine_args(), exchange=hub.bind(r),
                                   plan=plan, core=CudaPartition, math_mode=math_mode)
+            assert e._pairs  # no zero delay: two steps per pair of launches
+            e.set_pair_mode(pairs)
             res[r] = _run(e, net)
             e.close()
         except BaseException as exc:
