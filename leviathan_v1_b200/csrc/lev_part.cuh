@@ -20,6 +20,10 @@
 //   5. send/recv to the peers;
 //   6. part_unpack_kernel: received theta(t+1) into the halo columns of ring
 //      slot t+1, before the next step reads it (a delay-0 edge reads it).
+// With no zero delay, two steps go per pair of launches instead: pair_kernel
+// (steps t and t+1 but the last integrate; partials of r(t+1)), 2.-6. for
+// step t+1, finish_kernel (the integrate of t+1; partials of r(t+2)), 2.-6.
+// for step t+2 -- the next pair reads halo slots t+2 and older only.
 // This replaces the reference's multi-GPU stub (leviathan_multigpu.cu:97-115,
 // whose pack/unpack kernels are never launched, and :218-238, which averages
 // per-GPU |r| on the host) and its partitioner, which drops every edge that
