@@ -143,6 +143,20 @@ class CpuPartitionCore:
         r_slot.numpy()[0] = r
         self.cur = (self.cur + 1) % self.bsi
 
+    # two steps per pair of launches: the same arithmetic in this stand-in
+    # (the second step runs whole in pair_finish, after g(t+1) is known and
+    # theta(t+1) went to the peers), so a partitioned pair run checks the
+    # order of the data plane: theta(t+1) must be packed before the finish
+    # overwrites it
+    def pairs_eligible(self):
+        return bool(self.dl.size == 0 or self.dl.min() > 0)
+
+    def pair_begin(self, dt, partials):
+        self.step_begin(dt, partials)
+
+    def pair_finish(self, dt, partials):
+        self.step_begin(dt, partials)
+
     def pack(self, idx, out):
         out.numpy()[:] = self.theta[idx.numpy()]
 

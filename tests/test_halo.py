@@ -115,7 +115,7 @@ def test_cpu_core_matches_fp64_oracle():
     assert np.abs(e.get_weights() - o.w).max() < 1e-4
 
 
-def _threads(net, world, core):
+def _threads(net, world, core, pairs=None):
     hub = ThreadExchange(world)
     plan = PartitionPlan(net.row_ptr, net.col_idx, world)
     res, errs = {}, []
@@ -124,6 +124,9 @@ def _threads(net, world, core):
         try:
             e = PartitionedEngine(r, world, *net.engine_args(), exchange=hub.bind(r),
                                   core=core, plan=plan)
+            res[f"pairs{r}"] = e._pairs
+            if pairs is not None:
+                e.set_pair_mode(pairs)
             res[r] = _run(e, net)
             e.close()
         except BaseException as exc:  # report, and release the others
@@ -149,12 +152,29 @@ def _check_equal(res, ref, world):
     np.testing.assert_array_equal(w, ref["w"])
 
 
-def test_threads_partitioned_equals_unpartitioned_cpu():
+@pytest.mark.parametrize("pairs", [True, False], ids=["pairs", "single"])
+def test_threads_partitioned_equals_unpartitioned_cpu(pairs):
     from halo_cpu_core import CpuPartitionCore
 
     net = _net()
     ref = _unpartitioned(net, CpuPartitionCore)
-    _check_equal(_threads(net, 4, CpuPartitionCore), ref, 4)
+    res = _threads(net, 4, CpuPartitionCore, pairs)
+    assert all(res[f"pairs{r}"] for r in range(4))  # no zero delay anywhere
+    _check_equal(res, ref, 4)
+
+
+def test_ranks_agree_on_pairs():
+    """One zero delay in rank 0's rows only: every rank steps one step per
+    launch (they issue the same collectives), and the run is unchanged."""
+    from halo_cpu_core import CpuPartitionCore
+
+    net = _net()
+    net.delays = net.delays.copy()
+    net.delays[5] = 0
+    ref = _unpartitioned(net, CpuPartitionCore)
+    res = _threads(net, 3, CpuPartitionCore)
+    assert not any(res[f"pairs{r}"] for r in range(3))
+    _check_equal(res, ref, 3)
 
 
 def _free_port():
