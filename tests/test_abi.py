@@ -120,6 +120,11 @@ def test_null_handle_calls_are_errors():
     assert lib.lev_step(None, C.c_float(0.05), None) == _lib.LEV_ERR_ARG
     assert lib.lev_step_n(None, C.c_float(0.05), 3, None) == _lib.LEV_ERR_ARG
     assert lib.lev_destroy(None) == _lib.LEV_OK
+    el = C.c_int32()
+    assert lib.lev_part_pairs(None, C.byref(el)) == _lib.LEV_ERR_ARG
+    buf = C.c_void_p(16)  # never dereferenced: the handle check comes first
+    assert lib.lev_part_pair_begin(None, C.c_float(0.05), buf) == _lib.LEV_ERR_ARG
+    assert lib.lev_part_pair_finish(None, C.c_float(0.05), buf) == _lib.LEV_ERR_ARG
 
 
 def test_python_engine_validates_sizes():
