@@ -75,6 +75,7 @@ def _ptr(a):
     (2, 256, None, "max_delay"),
     (2, -1, None, "max_delay"),
     (2, 5, np.array([1, 1, 2], np.int32), "row_ptr[0]"),
+    (2, 5, np.array([0, 1, -1], np.int32), "row_ptr[N] is negative"),
 ])
 def test_create_rejects_bad_arguments_before_any_device_work(N, max_delay, rp_fix, msg):
     """Scalar arguments and the ends of row_ptr.  A decreasing row_ptr is
