@@ -390,6 +390,28 @@ def test_batch_equals_individual_engines():
     be.close()
 
 
+def test_batch_with_an_edgeless_network():
+    """A network without edges between two with edges: the device packing
+    writes nothing for it and the neighbours' slices stay in place."""
+    from leviathan_v1_b200.graphs import Network, init_state
+
+    a = make_network(900, 8, 0.1, 12, seed=7)
+    rp = np.zeros(301, np.int32)
+    st = init_state(rp, 5, 9)
+    empty = Network(300, 5, rp, np.zeros(0, np.int32), st["delays"], st["weights"],
+                    st["theta"], st["theta_hat"], st["omega"])
+    c = make_network(1500, 12, 0.1, 20, seed=8)
+    nets = [a, empty, c]
+    be = BatchEngine([n.as_dict() for n in nets])
+    rb = be.step_n(DT, 40)
+    for i, n in enumerate(nets):
+        e = LeviathanEngine(*n.engine_args())
+        np.testing.assert_array_equal(rb[:, i], e.step_n(DT, 40))
+        np.testing.assert_array_equal(be.get_theta(i), e.get_theta())
+        e.close()
+    be.close()
+
+
 @pytest.mark.parametrize("N,k,md,ctrl", [(1000, 20, 50, 1), (700, 8, 10, 0),
                                          (4096, 32, 64, 1), (3000, 12, 0, 1),
                                          (16000, 8, 8, 1)])
